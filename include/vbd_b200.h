@@ -1,0 +1,162 @@
+/*
+ * vbd_b200.h -- C ABI of the B200 Vertex Block Descent solver (libvbd_b200.so).
+ *
+ * Plain C types only: pointers to host arrays plus sizes, an opaque handle and
+ * integer status codes.  Every array argument is a HOST array; the library
+ * copies it to the GPU and keeps the solver state resident in device memory.
+ * Positions are exchanged in the caller's original vertex order as float64
+ * [n_vertices][3], like the reference's wp.vec3d arrays.
+ *
+ * The entry points replace the reference solver's Python interface
+ * (mmichelis/WarpVBD, src/vbd_solver.py):
+ *
+ *   vbd_create          VBDSolver.__init__            vbd_solver.py:366-498
+ *   vbd_step            VBDSolver.step                vbd_solver.py:509-612
+ *   vbd_reset           VBDSolver.reset               vbd_solver.py:501-506
+ *   vbd_get_positions   new_positions.numpy()         vbd_solver.py:612 (returned array)
+ *   vbd_set_positions   step(positions, ...) argument vbd_solver.py:535
+ *   vbd_get_color_groups  VBDSolver.color_groups      vbd_solver.py:476-483
+ *   vbd_graph_coloring  compute_adjacency_dict + graph_coloring  coloring.py:24-72
+ *   vbd_create_batched / vbd_step_batched
+ *                       the reference batches by concatenating meshes into one
+ *                       solver (examples/run_mass_spring_parallel.py:40-58,
+ *                       one global convergence test); here each environment
+ *                       keeps its own convergence test and iteration count.
+ *
+ * Threading: one CUDA stream per handle; a handle is not thread-safe.
+ */
+#ifndef VBD_B200_H
+#define VBD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct vbd_solver vbd_solver;
+
+/* ---- status codes ------------------------------------------------------ */
+#define VBD_OK 0
+/* the sweep loop reached max_iter without meeting the tolerance (the
+ * reference prints a warning, vbd_solver.py:581-582); results are valid */
+#define VBD_NOT_CONVERGED 1
+#define VBD_ERR_INVALID_ARG (-1)
+#define VBD_ERR_CUDA (-2)
+#define VBD_ERR_SINGULAR_DM (-3)     /* a tet with zero rest volume */
+#define VBD_ERR_TOO_MANY_COLORS (-4) /* greedy colouring needs > 256 colours (coloring.py:50) */
+#define VBD_ERR_NONFINITE (-5)       /* NaN / Inf appeared in the iterate */
+#define VBD_ERR_TIMEOUT (-6)         /* a bounded device-side wait gave up */
+#define VBD_ERR_NO_DEVICE (-7)
+#define VBD_ERR_UNSUPPORTED (-8)     /* e.g. an environment too large for block mode */
+
+/* ---- flags --------------------------------------------------------------- */
+#define VBD_MATERIAL_SNH 0x0  /* Stable Neo-Hookean, vbd_solver.py:107-124 */
+#define VBD_MATERIAL_STVK 0x1 /* St. Venant-Kirchhoff, vbd_solver.py:127-144 */
+#define VBD_PRECISION_FP32 0x00  /* fp32 state and arithmetic */
+#define VBD_PRECISION_FP64 0x10  /* fp64 state and arithmetic */
+/* fp64 positions / velocities, fp32 per-tet arithmetic on fp64-formed
+ * neighbour offsets: resolves position updates far below a 1e-7 m tolerance
+ * at metre-scale displacements, which an fp32 state cannot */
+#define VBD_PRECISION_MIXED 0x20
+#define VBD_MODE_AUTO 0x000
+#define VBD_MODE_BLOCK 0x100    /* one thread block per environment runs the whole step */
+#define VBD_MODE_GRAPH 0x200    /* per-colour kernels looped by a CUDA-graph conditional node */
+#define VBD_MODE_HOSTLOOP 0x300 /* per-colour kernels, the host reads the convergence test each sweep */
+#define VBD_MODE_MASK 0xF00
+#define VBD_ORDER_INDEX 0x1000  /* keep ascending vertex index inside a colour (default: by valence) */
+/* fail a step instead of taking the guarded fallback when a 3x3 block is not
+ * positive definite (the reference would produce NaN there) */
+#define VBD_STRICT_SPD 0x2000
+
+/* ---- library / device --------------------------------------------------- */
+int vbd_version(void);
+const char* vbd_status_string(int status);
+/* Text of the last error raised on the calling thread. */
+const char* vbd_last_error_message(void);
+int vbd_device_count(void);
+
+/* Greedy vertex colouring of the tet 1-ring in vertex index order
+ * (coloring.py:24-72).  coloring_out must hold max(tets)+1 entries; that
+ * count is written to *n_vertices_out and the colour count to *n_colors_out. */
+int vbd_graph_coloring(const int32_t* tets, int n_tets, int32_t* coloring_out,
+                       int* n_vertices_out, int* n_colors_out);
+
+/* ---- solver ------------------------------------------------------------ */
+/* VBDSolver.__init__ (vbd_solver.py:367-498).
+ *   rest_positions  float64 [n_vertices][3]   initial_positions
+ *   tets            int32   [n_tets][4]       elements
+ *   densities, youngs_modulus, poissons_ratio float64 [n_tets]
+ *   active_mask     uint8   [n_vertices], NULL = all active
+ *   damping_coefficient, gravity[3]
+ *   coloring        int32   [max(tets)+1] colour per vertex, NULL = computed
+ *   flags           VBD_MATERIAL_* | VBD_PRECISION_* | VBD_MODE_* | ...
+ *   tpv             lanes per vertex (1,2,4,8,16,32), 0 = pick automatically
+ *   block_threads   threads per block, 0 = pick automatically
+ *   device          CUDA device ordinal */
+int vbd_create(const double* rest_positions, int n_vertices, const int32_t* tets, int n_tets,
+               const double* densities, const double* youngs_modulus,
+               const double* poissons_ratio, const uint8_t* active_mask,
+               double damping_coefficient, const double* gravity, const int32_t* coloring,
+               int flags, int tpv, int block_threads, int device, vbd_solver** out);
+
+/* n_env independent environments concatenated: environment e owns vertices
+ * [env_vertex_offset[e], env_vertex_offset[e+1]) and tets
+ * [env_tet_offset[e], env_tet_offset[e+1]) (both arrays hold n_env+1
+ * entries); tets use concatenated vertex ids and must stay inside their
+ * environment.  Each environment is coloured on its own, which gives the same
+ * colours as colouring the concatenation (the environments are disjoint). */
+int vbd_create_batched(const double* rest_positions, int n_vertices, const int32_t* tets,
+                       int n_tets, const double* densities, const double* youngs_modulus,
+                       const double* poissons_ratio, const uint8_t* active_mask,
+                       double damping_coefficient, const double* gravity,
+                       const int32_t* env_vertex_offset, const int32_t* env_tet_offset,
+                       int n_env, int flags, int tpv, int block_threads, int device,
+                       vbd_solver** out);
+
+void vbd_destroy(vbd_solver* s);
+
+/* VBDSolver.reset (vbd_solver.py:501-506): positions back to rest, velocity 0 */
+int vbd_reset(vbd_solver* s);
+
+/* One implicit-Euler step of every environment (vbd_solver.py:509-612):
+ * inertia guess, sweeps over the colours until max |dx_x+dx_y+dx_z| < tol or
+ * max_iter sweeps, then v = (x_new - x_old)/dt.  With iterations_out != NULL
+ * the call blocks and writes the sweep count (per environment for the batched
+ * form); with NULL it only enqueues the work on the solver's stream.
+ * tol_per_env (batched only) may be NULL to use tol everywhere. */
+int vbd_step(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out);
+int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per_env,
+                     int max_iter, int* iterations_out);
+
+/* Wait for the enqueued work; returns the status of the last step. */
+int vbd_sync(vbd_solver* s);
+/* Sweep counts of the last step, n_env entries. */
+int vbd_get_iterations(vbd_solver* s, int* iterations_out);
+
+int vbd_get_positions(vbd_solver* s, double* positions_out);
+int vbd_set_positions(vbd_solver* s, const double* positions);
+int vbd_get_velocities(vbd_solver* s, double* velocities_out);
+int vbd_set_velocities(vbd_solver* s, const double* velocities);
+
+/* Reference-layout colour table: int32 [n_colors][max_group] of original
+ * vertex ids, -1 padded (vbd_solver.py:476-483).  Pass table = NULL to query
+ * the sizes first.  Batched solvers report the first environment. */
+int vbd_get_color_groups(vbd_solver* s, int32_t* table, int* n_colors, int* max_group);
+
+/* Sizes and the configuration the solver runs with. */
+typedef struct vbd_info_t {
+  int n_vertices, n_tets, n_env, n_colors, max_valence;
+  int mode, tpv, block_threads, precision, material;
+  long long n_slots, n_slot_records; /* incident (vertex, tet) pairs; padded records */
+  long long device_bytes;
+} vbd_info_t;
+int vbd_get_info(vbd_solver* s, vbd_info_t* info);
+
+/* The CUDA stream (cudaStream_t) all of the solver's work is enqueued on. */
+void* vbd_get_stream(vbd_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VBD_B200_H */

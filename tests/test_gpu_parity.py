@@ -1,0 +1,164 @@
+"""CUDA solver against the FP64 oracle (GPU tests, through the C ABI).
+
+Tolerances (fp32 solver vs FP64 oracle, same mesh / material / steps):
+  * every vertex position within 1e-5 of the bounding-box diagonal;
+  * tip-face mean displacement within 1e-5 relative (1e-4 for the shorter
+    StVK / damping / batched runs is not needed: the same 1e-5 is used);
+  * the FP64 device build within 1e-9 of the diagonal.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from warpvbd_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-5     # x bbox diagonal
+TIP_TOL = 1e-5     # relative
+
+
+def _diag(X):
+    return float(np.linalg.norm(X.max(0) - X.min(0)))
+
+
+def _tip_disp(x, s):
+    return (x[s.tip] - s.vertices[s.tip]).mean(axis=0)
+
+
+def run_pair(s, steps, material="snh", kd=0.0, precision="mixed", mode="auto", tol=1e-7,
+             max_iter=1000, dt=1e-3, **kw):
+    from warpvbd_b200 import VBDSolver
+    gpu = VBDSolver(**s.solver_kwargs(), damping_coefficient=kd, dx_tol=tol, max_iter=max_iter,
+                    material=material, precision=precision, mode=mode, **kw)
+    orc = oracle.OracleSolver(**s.solver_kwargs(), damping_coefficient=kd, dx_tol=tol,
+                              max_iter=max_iter, material=material, guarded=True)
+    its_g, its_o, worst = [], [], 0.0
+    D = _diag(s.vertices)
+    for k in range(steps):
+        xg = gpu.step(gpu.old_positions, dt).numpy()
+        xo = orc.step(None, dt)
+        its_g.append(gpu.last_iterations)
+        its_o.append(orc.last_iterations)
+        worst = max(worst, np.abs(xg - xo).max() / D)
+    return gpu, orc, xg, xo, np.array(its_g), np.array(its_o), worst
+
+
+@pytest.mark.parametrize("mode", ["block", "graph", "hostloop"])
+def test_cantilever_20x2x2_300_steps(mode):
+    s = scenes.cantilever(20)
+    steps = 300 if mode != "hostloop" else 60
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, steps, mode=mode)
+    assert gpu.info()["mode"] == {"block": 0x100, "graph": 0x200, "hostloop": 0x300}[mode]
+    assert worst < POS_TOL, worst
+    dg, do = _tip_disp(xg, s), _tip_disp(xo, s)
+    rel = np.linalg.norm(dg - do) / np.linalg.norm(do)
+    assert rel < TIP_TOL, (rel, dg, do)
+    assert np.abs(ig - io).max() <= 2, (ig, io)
+    assert np.array_equal(xg[~s.active], s.vertices[~s.active])
+
+
+def test_pure_fp32_state_drift_is_bounded():
+    """All-fp32 state: the displacement's own rounding (ulp 6e-8 m at 0.5 m)
+    feeds the Newton step, so the trajectory drifts further from FP64 than the
+    default mixed mode; bounded at 1e-4 of the diagonal over 300 steps."""
+    s = scenes.cantilever(20)
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 300, precision="fp32", mode="block")
+    assert worst < 1e-4, worst
+
+
+def test_fp64_device_build_matches_oracle_tightly():
+    s = scenes.cantilever(20)
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, precision="fp64", mode="block")
+    assert worst < 1e-9, worst
+    assert np.array_equal(ig, io)
+
+
+def test_fp64_graph_mode():
+    s = scenes.cantilever(40)
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 20, precision="fp64", mode="graph")
+    assert worst < 1e-9, worst
+    assert np.array_equal(ig, io)
+
+
+def test_stvk_cantilever():
+    s = scenes.cantilever(20)
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, material="stvk", mode="block")
+    assert worst < POS_TOL, worst
+    assert orc.guard_hits == 0
+
+
+def test_reference_default_damping():
+    s = scenes.cantilever(20)
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, kd=1.0, mode="block")
+    assert worst < POS_TOL, worst
+
+
+def test_mass_spring_11_20():
+    s = scenes.mass_spring(11, 20)
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, mode="block")
+    assert worst < POS_TOL, worst
+    dg, do = _tip_disp(xg, s), _tip_disp(xo, s)
+    assert np.linalg.norm(dg - do) / np.linalg.norm(do) < TIP_TOL
+
+
+def test_cantilever_40_graph_vs_block_vs_oracle():
+    s = scenes.cantilever(40)
+    _, _, xg, xo, ig, io, worst = run_pair(s, 30, mode="graph")
+    assert worst < POS_TOL, worst
+    _, _, xb, _, ib, _, worst_b = run_pair(s, 30, mode="block")
+    assert worst_b < POS_TOL, worst_b
+
+
+def test_batched_uneven_envs_match_per_env_oracle():
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(5, seed=11)
+    b = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000)
+    orcs = [oracle.OracleSolver(**e.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7,
+                                max_iter=1000, guarded=True) for e in envs]
+    for k in range(30):
+        its = b.step(1e-3)
+        x = b.positions()
+        for e, (env, o) in enumerate(zip(envs, orcs)):
+            xo = o.step(None, 1e-3)
+            xe = x[b.env_slice(e)]
+            assert np.abs(xe - xo).max() / _diag(env.vertices) < POS_TOL
+            assert abs(int(its[e]) - o.last_iterations) <= 2
+    assert len(set(its.tolist())) >= 1
+
+
+def test_step_api_semantics():
+    from warpvbd_b200 import VBDSolver
+    s = scenes.cantilever(20)
+    sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000)
+    x1 = sol.step(sol.old_positions, 1e-3)
+    a1 = x1.numpy()
+    v1 = sol.old_velocities.numpy()
+    assert np.allclose(v1, (a1 - s.vertices) / 1e-3, atol=1e-6)
+    x2 = sol.step(sol.old_positions, 1e-3)
+    with pytest.raises(RuntimeError):
+        x1.numpy()                         # overwritten by the second step
+    # stepping from an explicit host array uploads it
+    sol.reset()
+    assert np.allclose(sol.old_positions.numpy(), s.vertices)
+    x = sol.step(a1, 1e-3).numpy()
+    assert np.isfinite(x).all()
+    # colour table in the reference layout
+    col = oracle.graph_coloring(s.tets)
+    table = sol.color_groups
+    for c in range(table.shape[0]):
+        assert np.array_equal(table[c][table[c] >= 0], np.nonzero(col == c)[0])
+    assert sol.adj_v2e.shape == (189, 20)
+
+
+def test_nonconvergence_warning_and_nonfinite(capsys):
+    from warpvbd_b200 import VBDSolver
+    s = scenes.cantilever(20)
+    sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=2)
+    sol.step(sol.old_positions, 1e-3)
+    assert sol.last_iterations == 2
+    assert "did not converge" in capsys.readouterr().out
+    bad = s.vertices.copy()
+    bad[50] = np.nan
+    with pytest.raises(FloatingPointError):
+        sol.step(bad, 1e-3)

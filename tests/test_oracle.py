@@ -1,0 +1,225 @@
+"""The FP64 oracle itself: per-tet derivatives against finite differences of
+the energy, the kernel's closed form against the oracle's literal matrix form,
+setup tables and step semantics against the reference (src/vbd_solver.py)."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from warpvbd_b200 import scenes
+from tests import kernel_math
+
+
+def _random_tet(rng, strain=0.2):
+    X4 = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float) * 0.05
+    X4 = X4 + rng.normal(scale=0.004, size=X4.shape)
+    A = np.eye(3) + rng.normal(scale=strain, size=(3, 3))
+    x4 = X4 @ A.T + rng.normal(scale=0.002, size=3)
+    return X4, x4
+
+
+def _inv_dm(X4):
+    Dm = np.stack([X4[0] - X4[3], X4[1] - X4[3], X4[2] - X4[3]], axis=1)
+    return np.linalg.inv(Dm), abs(np.linalg.det(Dm)) / 6.0
+
+
+@pytest.mark.parametrize("material", [oracle.SNH, oracle.STVK])
+def test_tet_gradient_hessian_finite_differences(material):
+    rng = np.random.default_rng(7)
+    mu, lam = 3.4e5, 3.1e6
+    for _ in range(20):
+        X4, x4 = _random_tet(rng)
+        inv, vol = _inv_dm(X4)
+        for a in range(4):
+            g, H = oracle.tet_grad_hess(material, x4, inv, mu, lam, vol, a)
+            h = 1e-7
+            gfd = np.zeros(3)
+            Hfd = np.zeros((3, 3))
+            for i in range(3):
+                xp, xm = x4.copy(), x4.copy()
+                xp[a, i] += h
+                xm[a, i] -= h
+                gfd[i] = (oracle.tet_energy(material, xp, inv, mu, lam, vol)
+                          - oracle.tet_energy(material, xm, inv, mu, lam, vol)) / (2 * h)
+                gp, _ = oracle.tet_grad_hess(material, xp, inv, mu, lam, vol, a)
+                gm, _ = oracle.tet_grad_hess(material, xm, inv, mu, lam, vol, a)
+                Hfd[:, i] = (gp - gm) / (2 * h)
+            scale = max(1.0, np.abs(g).max())
+            assert np.allclose(g, gfd, rtol=1e-5, atol=1e-6 * scale)
+            assert np.allclose(H, Hfd, rtol=1e-5, atol=1e-5 * np.abs(H).max())
+            assert np.allclose(H, H.T, rtol=1e-12, atol=1e-9 * np.abs(H).max())
+
+
+@pytest.mark.parametrize("material", ["snh", "stvk"])
+def test_kernel_closed_form_matches_reference_formulation(material):
+    """The CUDA kernel's G-form (no F^-1, no cancellation) equals the
+    reference's trace formulation (vbd_solver.py:101-144)."""
+    rng = np.random.default_rng(11)
+    mu, lam = 3.4e5, 3.1e6
+    mat = {"snh": oracle.SNH, "stvk": oracle.STVK}[material]
+    for strain in (1e-4, 0.05, 0.3):
+        for _ in range(10):
+            X4, x4 = _random_tet(rng, strain)
+            inv, vol = _inv_dm(X4)
+            for a in range(4):
+                g_ref, H_ref = oracle.tet_grad_hess(mat, x4, inv, mu, lam, vol, a)
+                g, H = kernel_math.slot_grad_hess(material, X4, x4, a, mu, lam)
+                sg = np.abs(H_ref).max() * 1e-3
+                assert np.allclose(g, g_ref, rtol=1e-7, atol=1e-9 * sg), (strain, a)
+                assert np.allclose(H, H_ref, rtol=1e-7, atol=1e-9 * np.abs(H_ref).max())
+
+
+def test_snh_hessian_block_positive_definite():
+    rng = np.random.default_rng(5)
+    for _ in range(50):
+        X4, x4 = _random_tet(rng, 0.4)
+        inv, vol = _inv_dm(X4)
+        _, H = oracle.tet_grad_hess(oracle.SNH, x4, inv, 3e5, 3e6, vol, rng.integers(4))
+        assert np.linalg.eigvalsh(H).min() > -1e-9 * np.abs(H).max()
+
+
+def test_rest_state_is_stress_free():
+    X4, _ = _random_tet(np.random.default_rng(0))
+    inv, vol = _inv_dm(X4)
+    for mat in (oracle.SNH, oracle.STVK):
+        g, _ = oracle.tet_grad_hess(mat, X4, inv, 3e5, 3e6, vol, 0)
+        assert np.abs(g).max() < 1e-8 * 3e6 * vol / 0.05
+
+
+def _c1(**kw):
+    s = scenes.cantilever(20)
+    o = oracle.OracleSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7,
+                            max_iter=1000, **kw)
+    return s, o
+
+
+def test_setup_tables_match_reference_layout(golden):
+    s, o = _c1()
+    col = golden["cantilever_20/coloring"]
+    table = o.color_groups
+    assert table.shape == (7, 54)
+    for c in range(7):
+        grp = table[c][table[c] >= 0]
+        assert np.array_equal(grp, np.nonzero(col == c)[0])   # ascending vertex ids
+    adj = o.adj_v2e
+    assert adj.shape == (189, 20)
+    for v in (0, 17, 100, 188):
+        inc = np.nonzero((s.tets == v).any(axis=1))[0]
+        assert np.array_equal(adj[v][adj[v] >= 0], inc)
+    d = o.element_data()
+    assert o.bad_dm == 0
+    assert np.allclose(d["volumes"].sum(), 1.0 * 0.1 * 0.1)
+    E, nu = 1e6, 0.45
+    assert np.allclose(d["lame_mus"], E / (2 * (1 + nu)))
+    assert np.allclose(d["lame_lambdas"], E * nu / ((1 + nu) * (1 - 2 * nu)))
+
+
+def test_step_semantics():
+    s, o = _c1()
+    x0 = s.vertices
+    x1 = o.step(None, 1e-3)
+    fixed = ~s.active
+    assert np.array_equal(x1[fixed], x0[fixed])          # fixed vertices never move
+    assert np.array_equal(o.old_positions, x1)           # old_positions = new (:610)
+    assert np.allclose(o.old_velocities, (x1 - x0) / 1e-3)  # (:609)
+    assert 1 <= o.last_iterations < 1000 and not o.warned
+    o.reset()
+    assert np.array_equal(o.old_positions, x0)
+    assert not o.old_velocities.any()
+
+
+def test_max_iter_warning_condition():
+    _, o = _c1()
+    o.step(None, 1e-3, max_iter=2)
+    assert o.last_iterations == 2 and o.warned     # i == max_iter - 1 (:581)
+    _, o = _c1()
+    o.step(None, 1e-3, dx_tol=1e3, max_iter=1)
+    assert o.last_iterations == 1 and o.warned      # converged on the last sweep still warns
+
+
+def test_first_steps_iterations_known():
+    """Pins the sweep counts of the 20x2x2 cantilever's first steps at tol 1e-7."""
+    _, o = _c1()
+    its = []
+    for _ in range(6):
+        o.step(None, 1e-3)
+        its.append(o.last_iterations)
+    assert its == [5, 6, 7, 8, 8, 8]
+
+
+def test_thread_count_does_not_change_results():
+    s = scenes.cantilever(20)
+    out = []
+    for n in (1, 4):
+        oracle.set_threads(n)
+        o = oracle.OracleSolver(**s.solver_kwargs(), damping_coefficient=0.5, dx_tol=1e-7,
+                                max_iter=1000)
+        for _ in range(3):
+            x = o.step(None, 1e-3)
+        out.append(x)
+    oracle.set_threads(oracle.max_threads())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_incremental_potential_gradient_matches_step_gradient():
+    s, o = _c1()
+    o.step(None, 1e-3)
+    rng = np.random.default_rng(2)
+    x = o.old_positions + rng.normal(scale=1e-4, size=(s.n_vertices, 3)) * s.active[:, None]
+    dt = 1e-3
+    for v in (30, 90, 150):
+        if not s.active[v]:
+            continue
+        g, _ = o.vertex_grad_hess(v, x, dt)
+        h = 1e-7
+        fd = np.zeros(3)
+        for i in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[v, i] += h
+            xm[v, i] -= h
+            fd[i] = (o.incremental_potential(xp, dt) - o.incremental_potential(xm, dt)) / (2 * h)
+        assert np.allclose(g, fd, rtol=1e-4, atol=1e-4 * np.abs(g).max())
+
+
+def test_guarded_mode_vs_reference_mode_on_spd_problem():
+    s = scenes.cantilever(20)
+    kw = dict(s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000)
+    a = oracle.OracleSolver(**kw, guarded=False)
+    b = oracle.OracleSolver(**kw, guarded=True)
+    for _ in range(3):
+        xa = a.step(None, 1e-3)
+        xb = b.step(None, 1e-3)
+    assert np.array_equal(xa, xb) and b.guard_hits == 0
+
+
+def test_numpy_twin_single_sweep():
+    """An independent pure-numpy restatement of one sweep (vbd_solver.py:537-574)
+    on a 3x1x1 beam equals the C oracle with max_iter=1."""
+    s = scenes.cantilever(3, 1, 1, length=0.3)
+    X, T = s.vertices, s.tets
+    rho, E, nu, dt = 1000.0, 1e6, 0.45, 1e-3
+    g = np.array([0, 0, -9.81])
+    o = oracle.OracleSolver(X, T, np.full(len(T), rho), np.full(len(T), E), np.full(len(T), nu),
+                            damping_coefficient=0.0, active_mask=s.active, dx_tol=1e-7)
+    x_or = o.step(None, dt, max_iter=1)
+    mu, lam = E / (2 * (1 + nu)), E * nu / ((1 + nu) * (1 - 2 * nu))
+    x = X.copy()
+    x[s.active] += g * dt * dt
+    table = o.color_groups
+    for c in range(table.shape[0]):
+        for v in table[c][table[c] >= 0]:
+            if not s.active[v]:
+                continue
+            G = np.zeros(3)
+            H = np.zeros((3, 3))
+            for t in np.nonzero((T == v).any(axis=1))[0]:
+                ids = T[t]
+                a = int(np.nonzero(ids == v)[0][0])
+                b_all, vol = kernel_math.shape_gradients(X[ids])
+                m = rho * vol / 4
+                G += m / dt ** 2 * (x[v] - X[v]) - m * g
+                H += m / dt ** 2 * np.eye(3)
+                ge, he = kernel_math.slot_grad_hess("snh", X[ids], x[ids], a, mu, lam)
+                G += ge
+                H += he
+            x[v] += np.linalg.solve(H, -G)
+    assert np.allclose(x, x_or, rtol=0, atol=1e-12)

@@ -1,0 +1,145 @@
+"""ctypes binding of libvbd_b200.so (the C ABI in include/vbd_b200.h).
+
+The library is built in-tree (``make -C warpvbd_b200/csrc``, or
+``warpvbd_b200.build()``).  There is no CPU fallback: importing a solver
+without the compiled library raises ``ImportError``.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvbd_b200.so")
+CSRC = os.path.join(_HERE, "csrc")
+
+# status codes
+OK = 0
+NOT_CONVERGED = 1
+ERR_INVALID_ARG = -1
+ERR_CUDA = -2
+ERR_SINGULAR_DM = -3
+ERR_TOO_MANY_COLORS = -4
+ERR_NONFINITE = -5
+ERR_TIMEOUT = -6
+ERR_NO_DEVICE = -7
+ERR_UNSUPPORTED = -8
+
+# flags
+MATERIAL_SNH = 0x0
+MATERIAL_STVK = 0x1
+PRECISION_FP32 = 0x00
+PRECISION_FP64 = 0x10
+PRECISION_MIXED = 0x20
+PRECISIONS = {"fp32": PRECISION_FP32, "mixed": PRECISION_MIXED, "fp64": PRECISION_FP64}
+MODE_AUTO = 0x000
+MODE_BLOCK = 0x100
+MODE_GRAPH = 0x200
+MODE_HOSTLOOP = 0x300
+ORDER_INDEX = 0x1000
+STRICT_SPD = 0x2000
+
+MODES = {"auto": MODE_AUTO, "block": MODE_BLOCK, "graph": MODE_GRAPH, "hostloop": MODE_HOSTLOOP}
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int32)
+_u8 = ctypes.POINTER(ctypes.c_uint8)
+_ip = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+
+
+class VBDInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "n_vertices", "n_tets", "n_env", "n_colors", "max_valence", "mode", "tpv",
+        "block_threads", "precision", "material")] + [
+        ("n_slots", ctypes.c_longlong), ("n_slot_records", ctypes.c_longlong),
+        ("device_bytes", ctypes.c_longlong)]
+
+
+# every entry point declared in include/vbd_b200.h: name -> (restype, argtypes)
+SIGNATURES = {
+    "vbd_version": (ctypes.c_int, []),
+    "vbd_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "vbd_last_error_message": (ctypes.c_char_p, []),
+    "vbd_device_count": (ctypes.c_int, []),
+    "vbd_graph_coloring": (ctypes.c_int, [_i, ctypes.c_int, _i, _ip, _ip]),
+    "vbd_create": (ctypes.c_int, [_d, ctypes.c_int, _i, ctypes.c_int, _d, _d, _d, _u8,
+                                  ctypes.c_double, _d, _i, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "vbd_create_batched": (ctypes.c_int, [_d, ctypes.c_int, _i, ctypes.c_int, _d, _d, _d, _u8,
+                                          ctypes.c_double, _d, _i, _i, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.POINTER(_vp)]),
+    "vbd_destroy": (None, [_vp]),
+    "vbd_reset": (ctypes.c_int, [_vp]),
+    "vbd_step": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip]),
+    "vbd_step_batched": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _d,
+                                        ctypes.c_int, _ip]),
+    "vbd_sync": (ctypes.c_int, [_vp]),
+    "vbd_get_iterations": (ctypes.c_int, [_vp, _ip]),
+    "vbd_get_positions": (ctypes.c_int, [_vp, _d]),
+    "vbd_set_positions": (ctypes.c_int, [_vp, _d]),
+    "vbd_get_velocities": (ctypes.c_int, [_vp, _d]),
+    "vbd_set_velocities": (ctypes.c_int, [_vp, _d]),
+    "vbd_get_color_groups": (ctypes.c_int, [_vp, _i, _ip, _ip]),
+    "vbd_get_info": (ctypes.c_int, [_vp, ctypes.POINTER(VBDInfo)]),
+    "vbd_get_stream": (_vp, [_vp]),
+}
+
+_lib = None
+
+
+def build(verbose=False):
+    """Compile libvbd_b200.so for sm_100a in place (nvcc, no GPU needed)."""
+    cmd = ["make", "-C", CSRC] + ([] if verbose else ["-s"])
+    subprocess.check_call(cmd)
+
+
+def load():
+    """Load the compiled library (raises ImportError if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is not built; run `make -C {CSRC}` (nvcc, sm_100a). "
+            "warpvbd_b200 has no CPU fallback.")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+class VBDError(RuntimeError):
+    def __init__(self, status, message=""):
+        self.status = status
+        super().__init__(f"{message} (status {status})" if message else f"status {status}")
+
+
+def check(status, what=""):
+    """Raise on negative status codes; return the code otherwise."""
+    if status < 0:
+        L = load()
+        msg = L.vbd_last_error_message().decode(errors="replace")
+        text = L.vbd_status_string(status).decode()
+        raise VBDError(status, f"{what}: {text}: {msg}".strip(": "))
+    return status
+
+
+def ptr(a, kind):
+    if a is None:
+        return None
+    return a.ctypes.data_as({"d": _d, "i": _i, "u8": _u8}[kind])
+
+
+def f64(a, shape=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    return a.reshape(shape) if shape is not None else a
+
+
+def i32(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))

@@ -1,0 +1,147 @@
+"""Many independent VBD environments stepped in one launch.
+
+The reference batches environments by concatenating their meshes into one
+``VBDSolver`` (mmichelis/WarpVBD examples/run_mass_spring_parallel.py:35-58):
+one colouring, one global convergence test, so every environment runs as many
+sweeps as the slowest.  Here the environments keep their own convergence test
+and sweep count: block mode gives each environment one thread block that runs
+its whole step (all sweeps and colours) with the environment's displacements
+in shared memory.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .vbd_solver import _host, _device_index
+
+
+class BatchedVBDSolver:
+    """``envs``: sequence of objects with ``vertices``, ``tets``, ``density``,
+    ``youngs``, ``poisson``, ``active`` (warpvbd_b200.scenes.Scene) or dicts
+    with the ``VBDSolver`` argument names."""
+
+    def __init__(self, envs, damping_coefficient=0.0, gravity=(0.0, 0.0, -9.81), dx_tol=1e-7,
+                 max_iter=1000, device="cuda", *, material="snh", precision="mixed",
+                 tpv=0, block_threads=0, order_index=False):
+        Xs, Ts, rho, E, nu, act = [], [], [], [], [], []
+        voff, toff = [0], [0]
+        for env in envs:
+            get = (lambda k, a: env[k]) if isinstance(env, dict) else (lambda k, a: getattr(env, a))
+            X = np.asarray(_host(get("initial_positions", "vertices")), np.float64).reshape(-1, 3)
+            t = np.asarray(_host(get("elements", "tets")), np.int64).reshape(-1, 4)
+            Xs.append(X)
+            Ts.append(t + voff[-1])
+            rho.append(np.asarray(_host(get("densities", "density")), np.float64))
+            E.append(np.asarray(_host(get("youngs_modulus", "youngs")), np.float64))
+            nu.append(np.asarray(_host(get("poissons_ratio", "poisson")), np.float64))
+            a = get("active_mask", "active")
+            act.append(np.ones(X.shape[0], bool) if a is None else np.asarray(_host(a), bool))
+            voff.append(voff[-1] + X.shape[0])
+            toff.append(toff[-1] + t.shape[0])
+        self.n_env = len(Xs)
+        self.env_vertex_offset = np.asarray(voff, np.int32)
+        self.env_tet_offset = np.asarray(toff, np.int32)
+        X = _lib.f64(np.concatenate(Xs))
+        tets = _lib.i32(np.concatenate(Ts))
+        rho, E, nu = (_lib.f64(np.concatenate(a)) for a in (rho, E, nu))
+        actu8 = np.ascontiguousarray(np.concatenate(act).astype(np.uint8))
+        g = _lib.f64(gravity, (3,))
+        flags = {"snh": _lib.MATERIAL_SNH, "stvk": _lib.MATERIAL_STVK}[material]
+        flags |= _lib.PRECISIONS[precision]
+        flags |= _lib.MODE_BLOCK
+        if order_index:
+            flags |= _lib.ORDER_INDEX
+        L = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(L.vbd_create_batched(
+            _lib.ptr(X, "d"), X.shape[0], _lib.ptr(tets, "i"), tets.shape[0], _lib.ptr(rho, "d"),
+            _lib.ptr(E, "d"), _lib.ptr(nu, "d"), actu8.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+            float(damping_coefficient), _lib.ptr(g, "d"), _lib.ptr(self.env_vertex_offset, "i"),
+            _lib.ptr(self.env_tet_offset, "i"), self.n_env, flags, int(tpv), int(block_threads),
+            _device_index(device), ctypes.byref(h)), "vbd_create_batched")
+        self._h = h
+        self.n_vertices = X.shape[0]
+        self.initial_positions = X.copy()
+        self.dx_tol = dx_tol
+        self.max_iter = max_iter
+        self.last_iterations = np.zeros(self.n_env, np.int32)
+        self.last_status = _lib.OK
+
+    def info(self):
+        inf = _lib.VBDInfo()
+        _lib.check(_lib.load().vbd_get_info(self._h, ctypes.byref(inf)))
+        return {n: getattr(inf, n) for n, _ in _lib.VBDInfo._fields_}
+
+    @property
+    def stream(self):
+        return _lib.load().vbd_get_stream(self._h)
+
+    def step(self, dt=1e-3, dx_tol=None, tol_per_env=None, max_iter=None, blocking=True):
+        """Step every environment; returns the per-environment sweep counts
+        (blocking) or None (enqueued only; see ``sync``)."""
+        L = _lib.load()
+        tol = self.dx_tol if dx_tol is None else dx_tol
+        mi = self.max_iter if max_iter is None else max_iter
+        tpe = None if tol_per_env is None else _lib.f64(tol_per_env, (self.n_env,))
+        if blocking:
+            it = np.zeros(self.n_env, np.int32)
+            st = L.vbd_step_batched(self._h, float(dt), float(tol), _lib.ptr(tpe, "d"), int(mi),
+                                    it.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+            self._after(st, it)
+            return it
+        _lib.check(L.vbd_step_batched(self._h, float(dt), float(tol), _lib.ptr(tpe, "d"),
+                                      int(mi), None), "vbd_step_batched")
+        return None
+
+    def sync(self):
+        L = _lib.load()
+        st = L.vbd_sync(self._h)
+        it = np.zeros(self.n_env, np.int32)
+        L.vbd_get_iterations(self._h, it.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        self._after(st, it)
+        return it
+
+    def _after(self, st, it):
+        self.last_status = st
+        self.last_iterations = it
+        if st == _lib.ERR_NONFINITE:
+            raise FloatingPointError("VBD step produced non-finite positions")
+        _lib.check(st, "vbd_step_batched")
+
+    def positions(self):
+        out = np.empty((self.n_vertices, 3))
+        _lib.check(_lib.load().vbd_get_positions(self._h, _lib.ptr(out, "d")))
+        return out
+
+    def velocities(self):
+        out = np.empty((self.n_vertices, 3))
+        _lib.check(_lib.load().vbd_get_velocities(self._h, _lib.ptr(out, "d")))
+        return out
+
+    def env_slice(self, e):
+        return slice(int(self.env_vertex_offset[e]), int(self.env_vertex_offset[e + 1]))
+
+    def set_state(self, positions=None, velocities=None):
+        L = _lib.load()
+        if positions is not None:
+            x = _lib.f64(positions, (self.n_vertices, 3))
+            _lib.check(L.vbd_set_positions(self._h, _lib.ptr(x, "d")))
+        if velocities is not None:
+            v = _lib.f64(velocities, (self.n_vertices, 3))
+            _lib.check(L.vbd_set_velocities(self._h, _lib.ptr(v, "d")))
+
+    def reset(self):
+        _lib.check(_lib.load().vbd_reset(self._h))
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.load().vbd_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

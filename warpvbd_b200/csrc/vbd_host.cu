@@ -1,0 +1,985 @@
+// Host side of libvbd_b200.so: mesh setup, device layout, the conditional
+// CUDA-graph sweep loop and the C ABI declared in include/vbd_b200.h.
+//
+// Setup restates VBDSolver.__init__ (mmichelis/WarpVBD src/vbd_solver.py:366-498)
+// natively: Lame parameters (:345-362), Dm^-1 / volume / mass per tet
+// (:295-343), the greedy colouring (src/coloring.py:24-72) and the
+// vertex -> tet adjacency (:485-498).  Instead of the reference's padded
+// [n_colors, max_group] colour table and [V, 20] adjacency it renumbers the
+// vertices colour by colour and stores one record per incident (vertex, tet)
+// pair in a SELL-32 layout (see vbd_internal.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vbd_b200.h"
+#include "vbd_internal.h"
+#include "vbd_launch.h"
+
+using namespace vbd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                  \
+  do {                                                                                  \
+    cudaError_t _e = (expr);                                                            \
+    if (_e != cudaSuccess)                                                              \
+      return fail(VBD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));    \
+  } while (0)
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count) {
+    n = count;
+    return cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (count ? count : 1));
+  }
+  cudaError_t upload(const std::vector<T>& h, cudaStream_t s) {
+    cudaError_t e = alloc(h.size());
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpyAsync(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s);
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Greedy colouring (coloring.py:24-72): vertices in index order, each takes
+// the smallest colour not used by an already-coloured vertex sharing a tet.
+// Vertex count = max(tets)+1.  Returns the colour count or -1 (> 256 colours).
+// ---------------------------------------------------------------------------
+int greedy_coloring(const int32_t* tets, int T, int nv, int32_t* col) {
+  std::vector<int> off(nv + 1, 0), inc(4 * (size_t)T);
+  for (int i = 0; i < 4 * T; ++i) off[tets[i] + 1]++;
+  for (int v = 0; v < nv; ++v) off[v + 1] += off[v];
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (int t = 0; t < T; ++t)
+    for (int q = 0; q < 4; ++q) inc[fill[tets[4 * t + q]]++] = t;
+  std::fill(col, col + nv, -1);
+  int ncol = 0;
+  uint8_t used[257];
+  for (int v = 0; v < nv; ++v) {
+    std::memset(used, 0, sizeof used);
+    for (int s = off[v]; s < off[v + 1]; ++s) {
+      const int32_t* e = tets + 4 * (size_t)inc[s];
+      for (int q = 0; q < 4; ++q) {
+        const int n = e[q];
+        if (n != v && col[n] >= 0) used[col[n]] = 1;
+      }
+    }
+    int c = 0;
+    while (c < 256 && used[c]) ++c;
+    if (c == 256) return -1;
+    col[v] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  return ncol;
+}
+
+struct TetData {
+  std::vector<double> b;  // [T][4][3] shape-function gradients
+  std::vector<double> p;  // [T][3] (V*mu, V*lambda, alpha)
+  std::vector<double> mass;
+};
+
+int build_tet_data(const double* X, const int32_t* tets, int T, const double* rho,
+                   const double* E, const double* nu, int material, TetData& td) {
+  td.b.assign((size_t)T * 12, 0.0);
+  td.p.assign((size_t)T * 3, 0.0);
+  td.mass.assign(T, 0.0);
+  for (int t = 0; t < T; ++t) {
+    const int32_t* e = tets + 4 * (size_t)t;
+    double D[9];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) D[r * 3 + c] = X[3 * (size_t)e[c] + r] - X[3 * (size_t)e[3] + r];
+    const double det = D[0] * (D[4] * D[8] - D[5] * D[7]) - D[1] * (D[3] * D[8] - D[5] * D[6]) +
+                       D[2] * (D[3] * D[7] - D[4] * D[6]);
+    if (!(det != 0.0) || !std::isfinite(det))
+      return fail(VBD_ERR_SINGULAR_DM, "tet " + std::to_string(t) + " has zero rest volume");
+    const double s = 1.0 / det;
+    double I[9];
+    I[0] = (D[4] * D[8] - D[5] * D[7]) * s;
+    I[1] = (D[2] * D[7] - D[1] * D[8]) * s;
+    I[2] = (D[1] * D[5] - D[2] * D[4]) * s;
+    I[3] = (D[5] * D[6] - D[3] * D[8]) * s;
+    I[4] = (D[0] * D[8] - D[2] * D[6]) * s;
+    I[5] = (D[2] * D[3] - D[0] * D[5]) * s;
+    I[6] = (D[3] * D[7] - D[4] * D[6]) * s;
+    I[7] = (D[1] * D[6] - D[0] * D[7]) * s;
+    I[8] = (D[0] * D[4] - D[1] * D[3]) * s;
+    double* b = &td.b[(size_t)t * 12];
+    for (int q = 0; q < 3; ++q)
+      for (int c = 0; c < 3; ++c) b[q * 3 + c] = I[q * 3 + c];  // row q of Dm^-1
+    for (int c = 0; c < 3; ++c) b[9 + c] = -(I[c] + I[3 + c] + I[6 + c]);
+    const double vol = std::fabs(det) / 6.0;
+    td.mass[t] = rho[t] * vol;
+    const double mu = E[t] / (2.0 * (1.0 + nu[t]));
+    const double lam = (E[t] * nu[t]) / ((1.0 + nu[t]) * (1.0 - 2.0 * nu[t]));
+    double* p = &td.p[(size_t)t * 3];
+    if (material == kSNH) {
+      const double mu2 = 4.0 * mu / 3.0, lam2 = lam + 5.0 * mu / 6.0;
+      p[0] = vol * mu2;
+      p[1] = vol * lam2;
+      p[2] = 1.0 + 0.75 * mu2 / lam2;
+    } else {
+      p[0] = vol * mu;
+      p[1] = vol * lam;
+      p[2] = 0.0;
+    }
+  }
+  return VBD_OK;
+}
+
+struct Layout {
+  std::vector<EnvInfo> env;
+  std::vector<ColorInfo> color;
+  std::vector<ChunkInfo> chunk;
+  std::vector<int4> rec_idx;
+  std::vector<double> rec_val;  // [block][plane][lane][4]
+  std::vector<int> valence;     // new id
+  std::vector<double> mass;     // new id
+  std::vector<int> new_of_old;
+  std::vector<int32_t> table0;  // env 0 colour table (original ids)
+  int table_colors = 0, table_max_group = 0;
+  int max_valence = 0, max_colors = 0, max_env_vertices = 0;
+  long long n_slots = 0;
+};
+
+int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8_t* active,
+                 const std::vector<int>& voff, const std::vector<int>& toff,
+                 const int32_t* coloring, const TetData& td, int tpv, bool order_index,
+                 Layout& L) {
+  const int n_env = (int)voff.size() - 1;
+  const int cpw = 32 / tpv;
+  L.new_of_old.assign(V, -1);
+  L.valence.assign(V, 0);
+  L.mass.assign(V, 0.0);
+  int block_count = 0;
+  for (int e = 0; e < n_env; ++e) {
+    const int vo = voff[e], vn = voff[e + 1] - voff[e];
+    const int to = toff[e], tn = toff[e + 1] - toff[e];
+    if (vn < 0 || tn < 0) return fail(VBD_ERR_INVALID_ARG, "environment offsets decrease");
+    std::vector<int32_t> lt(4 * (size_t)tn);
+    int nv_col = 0;
+    for (size_t i = 0; i < lt.size(); ++i) {
+      const int g = tets[4 * (size_t)to + i];
+      if (g < vo || g >= vo + vn)
+        return fail(VBD_ERR_INVALID_ARG, "tet " + std::to_string(to + i / 4) +
+                                             " references a vertex outside its environment");
+      lt[i] = g - vo;
+      nv_col = std::max(nv_col, lt[i] + 1);
+    }
+    // colours of the local vertices (-1: not coloured)
+    std::vector<int32_t> col(vn, -1);
+    int ncol = 0;
+    if (coloring && n_env == 1) {
+      for (int v = 0; v < nv_col; ++v) {
+        col[v] = coloring[v];
+        if (col[v] < 0 || col[v] >= 256) return fail(VBD_ERR_INVALID_ARG, "bad colour value");
+        ncol = std::max(ncol, col[v] + 1);
+      }
+      // vertices of one colour must not share a tet, or their updates race
+      for (int t = 0; t < tn; ++t)
+        for (int a = 0; a < 4; ++a)
+          for (int b = a + 1; b < 4; ++b)
+            if (col[lt[4 * (size_t)t + a]] == col[lt[4 * (size_t)t + b]])
+              return fail(VBD_ERR_INVALID_ARG,
+                          "coloring gives two vertices of tet " + std::to_string(t) +
+                              " the same colour");
+    } else if (tn > 0) {
+      ncol = greedy_coloring(lt.data(), tn, nv_col, col.data());
+      if (ncol < 0) return fail(VBD_ERR_TOO_MANY_COLORS, "Exceeded maximum number of colors");
+    }
+    // incident tets, ascending tet id
+    std::vector<int> off(vn + 1, 0), inc(4 * (size_t)tn), loc(4 * (size_t)tn);
+    for (size_t i = 0; i < lt.size(); ++i) off[lt[i] + 1]++;
+    for (int v = 0; v < vn; ++v) off[v + 1] += off[v];
+    {
+      std::vector<int> fill(off.begin(), off.end() - 1);
+      for (int t = 0; t < tn; ++t)
+        for (int q = 0; q < 4; ++q) {
+          const int v = lt[4 * (size_t)t + q];
+          inc[fill[v]] = t;
+          loc[fill[v]] = q;
+          fill[v]++;
+        }
+    }
+    // colour table of environment 0 in the reference layout
+    if (e == 0) {
+      std::vector<std::vector<int>> groups(ncol);
+      for (int v = 0; v < nv_col; ++v)
+        if (col[v] >= 0) groups[col[v]].push_back(vo + v);
+      int mg = 0;
+      for (auto& g : groups) mg = std::max(mg, (int)g.size());
+      L.table_colors = ncol;
+      L.table_max_group = mg;
+      L.table0.assign((size_t)ncol * mg, -1);
+      for (int c = 0; c < ncol; ++c)
+        for (size_t i = 0; i < groups[c].size(); ++i) L.table0[(size_t)c * mg + i] = groups[c][i];
+    }
+    // classify and order
+    std::vector<std::vector<int>> solved(ncol);
+    std::vector<int> freev, fixedv;
+    for (int v = 0; v < vn; ++v) {
+      const bool act = active ? active[vo + v] != 0 : true;
+      const int k = off[v + 1] - off[v];
+      if (!act)
+        fixedv.push_back(v);
+      else if (col[v] >= 0 && k > 0)
+        solved[col[v]].push_back(v);
+      else
+        freev.push_back(v);
+      L.max_valence = std::max(L.max_valence, k);
+    }
+    EnvInfo ei{};
+    ei.vbase = vo;
+    ei.nv = vn;
+    ei.cbase = (int)L.color.size();
+    int next = 0;
+    std::vector<int> new_local(vn, -1);
+    for (int c = 0; c < ncol; ++c) {
+      auto& g = solved[c];
+      if (g.empty()) continue;
+      if (!order_index)
+        std::stable_sort(g.begin(), g.end(), [&](int a, int b) {
+          return (off[a + 1] - off[a]) > (off[b + 1] - off[b]);
+        });
+      ColorInfo ci{};
+      ci.vbegin = vo + next;
+      for (int v : g) new_local[v] = next++;
+      ci.vend = vo + next;
+      ci.chunk_begin = (int)L.chunk.size();
+      const int ng = (int)g.size();
+      for (int base = 0; base < ng; base += cpw) {
+        int kmax = 0;
+        for (int i = base; i < std::min(ng, base + cpw); ++i)
+          kmax = std::max(kmax, off[g[i] + 1] - off[g[i]]);
+        ChunkInfo ch{};
+        ch.block = block_count;
+        ch.steps = (kmax + tpv - 1) / tpv;
+        block_count += ch.steps;
+        L.chunk.push_back(ch);
+      }
+      ci.chunk_end = (int)L.chunk.size();
+      L.color.push_back(ci);
+    }
+    ei.nsolved = next;
+    for (int v : freev) new_local[v] = next++;
+    ei.nact = next;
+    for (int v : fixedv) new_local[v] = next++;
+    ei.ncolors = (int)L.color.size() - ei.cbase;
+    L.env.push_back(ei);
+    L.max_colors = std::max(L.max_colors, ei.ncolors);
+    L.max_env_vertices = std::max(L.max_env_vertices, vn);
+    for (int v = 0; v < vn; ++v) {
+      const int gnew = vo + new_local[v];
+      L.new_of_old[vo + v] = gnew;
+      L.valence[gnew] = off[v + 1] - off[v];
+      double m = 0.0;
+      for (int s = off[v]; s < off[v + 1]; ++s) m += td.mass[to + inc[s]] / 4.0;
+      L.mass[gnew] = m;
+    }
+    // slot records
+    L.rec_idx.resize((size_t)block_count * 32, make_int4(0, 0, 0, 0));
+    L.rec_val.resize((size_t)block_count * 32 * 12, 0.0);
+    // fill records by walking solved vertices in new order
+    std::vector<int> old_of_new_local(vn);
+    for (int v = 0; v < vn; ++v) old_of_new_local[new_local[v]] = v;
+    for (int ci_i = ei.cbase; ci_i < ei.cbase + ei.ncolors; ++ci_i) {
+      const ColorInfo ci = L.color[ci_i];
+      for (int q = ci.chunk_begin; q < ci.chunk_end; ++q) {
+        const ChunkInfo ch = L.chunk[q];
+        for (int lane = 0; lane < 32; ++lane) {
+          const int vi = lane / tpv, sub = lane % tpv;
+          const int gv = ci.vbegin + (q - ci.chunk_begin) * cpw + vi;
+          if (gv >= ci.vend) continue;
+          const int ov = old_of_new_local[gv - vo];
+          const int k = off[ov + 1] - off[ov];
+          for (int s = 0; s < ch.steps; ++s) {
+            const int j = s * tpv + sub;
+            if (j >= k) break;
+            const int t = to + inc[off[ov] + j];
+            const int a = loc[off[ov] + j];
+            const size_t blk = (size_t)ch.block + s;
+            int ids[3];
+            const double* bt = &td.b[(size_t)t * 12];
+            const double* pt = &td.p[(size_t)t * 3];
+            double* val = &L.rec_val[(blk * 3 * 32) * 4];
+            int n = 0;
+            for (int qq = 0; qq < 4; ++qq) {
+              if (qq == a) continue;
+              const int other_old = tets[4 * (size_t)t + qq] - vo;
+              ids[n] = new_local[other_old];
+              double* pv = val + ((size_t)n * 32 + lane) * 4;
+              pv[0] = bt[qq * 3 + 0];
+              pv[1] = bt[qq * 3 + 1];
+              pv[2] = bt[qq * 3 + 2];
+              pv[3] = pt[n];
+              ++n;
+            }
+            L.rec_idx[blk * 32 + lane] = make_int4(ids[0], ids[1], ids[2], 0);
+            L.n_slots++;
+          }
+        }
+      }
+    }
+  }
+  return VBD_OK;
+}
+
+}  // namespace
+
+struct vbd_solver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool fp64 = false;     // arithmetic and slot records in double
+  bool state64 = false;  // state vectors in double
+  int prec = 0;          // 0 fp32, 1 mixed (fp64 state, fp32 arithmetic), 2 fp64
+  int material = 0, mode = 0, tpv = 4, threads = 256, flags = 0;
+  int V = 0, T = 0, n_env = 0;
+  double kd = 0.0, g[3] = {0, 0, 0};
+  size_t real4_bytes = 16;
+  Layout L;
+  size_t smem_bytes = 0;
+  long long n_records = 0;
+  long long device_bytes = 0;
+  // device
+  DevBuf<EnvInfo> d_env;
+  DevBuf<ColorInfo> d_color;
+  DevBuf<ChunkInfo> d_chunk;
+  DevBuf<int4> d_rec_idx;
+  DevBuf<unsigned char> d_rec_val;
+  DevBuf<int> d_valence, d_map, d_iters;
+  DevBuf<unsigned> d_status;
+  DevBuf<unsigned char> d_u, d_ut, d_up, d_vel;
+  DevBuf<double> d_X, d_io, d_tol;
+  DevBuf<StepParams> d_params;
+  DevBuf<LoopControl> d_ctl;
+  // pinned host
+  int* h_iters = nullptr;
+  unsigned* h_status = nullptr;
+  StepParams* h_params = nullptr;
+  LoopControl* h_ctl = nullptr;
+  StepParams cur_params{};
+  bool params_valid = false;
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int last_status = VBD_OK;
+  bool pending = false;
+
+  DevMesh mesh() const {
+    DevMesh m{};
+    m.env = d_env.p;
+    m.color = d_color.p;
+    m.chunk = d_chunk.p;
+    m.rec_idx = d_rec_idx.p;
+    m.rec_val = d_rec_val.p;
+    m.valence = d_valence.p;
+    m.u = d_u.p;
+    m.ut = d_ut.p;
+    m.up = d_up.p;
+    m.vel = d_vel.p;
+    m.iters = d_iters.p;
+    m.status = d_status.p;
+    m.n_env = n_env;
+    m.n_vertices = V;
+    return m;
+  }
+};
+
+namespace {
+
+void free_solver(vbd_solver* s) {
+  if (!s) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->d_env.release();
+  s->d_color.release();
+  s->d_chunk.release();
+  s->d_rec_idx.release();
+  s->d_rec_val.release();
+  s->d_valence.release();
+  s->d_map.release();
+  s->d_iters.release();
+  s->d_status.release();
+  s->d_u.release();
+  s->d_ut.release();
+  s->d_up.release();
+  s->d_vel.release();
+  s->d_X.release();
+  s->d_io.release();
+  s->d_tol.release();
+  s->d_params.release();
+  s->d_ctl.release();
+  if (s->h_iters) cudaFreeHost(s->h_iters);
+  if (s->h_status) cudaFreeHost(s->h_status);
+  if (s->h_params) cudaFreeHost(s->h_params);
+  if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  cudaSetDevice(prev);
+  delete s;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int d) {
+    cudaGetDevice(&prev);
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int create_impl(const double* X, int V, const int32_t* tets, int T, const double* rho,
+                const double* E, const double* nu, const uint8_t* active, double kd,
+                const double* gravity, const int32_t* coloring, const std::vector<int>& voff,
+                const std::vector<int>& toff, int flags, int tpv, int threads, int device,
+                vbd_solver** out) {
+  if (!out) return fail(VBD_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (V <= 0 || T < 0 || !X || (T > 0 && (!tets || !rho || !E || !nu)))
+    return fail(VBD_ERR_INVALID_ARG, "empty mesh or NULL array");
+  for (size_t i = 0; i < 4 * (size_t)T; ++i)
+    if (tets[i] < 0 || tets[i] >= V)
+      return fail(VBD_ERR_INVALID_ARG, "tet vertex id out of range");
+  if (tpv != 0 && tpv != 1 && tpv != 2 && tpv != 4 && tpv != 8 && tpv != 16 && tpv != 32)
+    return fail(VBD_ERR_INVALID_ARG, "tpv must be 1, 2, 4, 8, 16 or 32");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(VBD_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(VBD_ERR_INVALID_ARG, "bad device ordinal");
+  DeviceGuard dg(device);
+
+  vbd_solver* s = new vbd_solver();
+  s->device = device;
+  s->flags = flags;
+  s->prec = (flags & VBD_PRECISION_FP64) ? 2 : ((flags & VBD_PRECISION_MIXED) ? 1 : 0);
+  s->fp64 = s->prec == 2;
+  s->state64 = s->prec >= 1;
+  s->material = (flags & VBD_MATERIAL_STVK) ? kStVK : kSNH;
+  s->V = V;
+  s->T = T;
+  s->n_env = (int)voff.size() - 1;
+  s->kd = kd;
+  for (int i = 0; i < 3; ++i) s->g[i] = gravity ? gravity[i] : (i == 2 ? -9.81 : 0.0);
+  s->real4_bytes = s->state64 ? 32 : 16;
+
+  TetData td;
+  int rc = build_tet_data(X, tets, T, rho, E, nu, s->material, td);
+  if (rc != VBD_OK) {
+    delete s;
+    return rc;
+  }
+  // mode / threads / tpv
+  int mode = flags & VBD_MODE_MASK;
+  // provisional environment size bound for the shared-memory check
+  int max_env_v = 0;
+  for (int e = 0; e < s->n_env; ++e) max_env_v = std::max(max_env_v, voff[e + 1] - voff[e]);
+  const size_t smem_need = (size_t)max_env_v * s->real4_bytes;
+  const bool fits = smem_need <= (size_t)env_kernel_max_smem();
+  if (mode == VBD_MODE_AUTO) {
+    if (s->n_env > 1)
+      mode = VBD_MODE_BLOCK;
+    else
+      mode = (fits && V <= 8192) ? VBD_MODE_BLOCK : VBD_MODE_GRAPH;
+  }
+  if (mode == VBD_MODE_BLOCK && !fits) {
+    delete s;
+    return fail(VBD_ERR_UNSUPPORTED, "an environment does not fit in shared memory for block mode");
+  }
+  if ((mode == VBD_MODE_GRAPH || mode == VBD_MODE_HOSTLOOP) && s->n_env != 1) {
+    delete s;
+    return fail(VBD_ERR_UNSUPPORTED, "graph / host-loop mode runs a single environment");
+  }
+  s->mode = mode;
+  const bool block_mode = mode == VBD_MODE_BLOCK;
+  if (threads == 0) threads = block_mode ? (s->n_env > 1 ? 256 : 512) : 256;
+  if (!block_mode) threads = 256;
+  if (threads % 32 || threads < 32 || threads > 512) {
+    delete s;
+    return fail(VBD_ERR_INVALID_ARG, "block_threads must be a multiple of 32 in [32, 512]");
+  }
+  s->threads = threads;
+  if (tpv == 0) {
+    if (block_mode && s->n_env == 1) {
+      // spread the largest colour over the block: lanes per vertex ~ threads / colour size
+      std::vector<int32_t> col(V, -1);
+      int nvc = 0;
+      for (size_t i = 0; i < 4 * (size_t)T; ++i) nvc = std::max(nvc, tets[i] + 1);
+      int ncol = coloring ? 0 : greedy_coloring(tets, T, nvc, col.data());
+      if (coloring) {
+        for (int v = 0; v < nvc; ++v) col[v] = coloring[v];
+        for (int v = 0; v < nvc; ++v) ncol = std::max(ncol, col[v] + 1);
+      }
+      std::vector<int> cnt(std::max(ncol, 1), 0);
+      for (int v = 0; v < nvc; ++v)
+        if (col[v] >= 0) cnt[col[v]]++;
+      const int mg = std::max(1, *std::max_element(cnt.begin(), cnt.end()));
+      tpv = 1;
+      while (tpv < 32 && mg * tpv * 2 <= threads) tpv *= 2;
+      if (tpv < 2) tpv = 2;
+    } else {
+      tpv = 4;  // batched environments and the grid-mode colour kernels
+    }
+  }
+  s->tpv = tpv;
+  rc = build_layout(X, V, tets, T, active, voff, toff, coloring, td, tpv,
+                    (flags & VBD_ORDER_INDEX) != 0, s->L);
+  if (rc != VBD_OK) {
+    delete s;
+    return rc;
+  }
+  s->smem_bytes = (size_t)s->L.max_env_vertices * s->real4_bytes;
+  s->n_records = (long long)s->L.rec_idx.size();
+
+  // ---- device upload --------------------------------------------------------
+  auto bad = [&](cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return false;
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return true;
+  };
+  int err = 0;
+  if (bad(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream")) err = 1;
+  cudaStream_t st = s->stream;
+  const Layout& L = s->L;
+  if (!err && bad(s->d_env.upload(L.env, st), "env")) err = 1;
+  if (!err && bad(s->d_color.upload(L.color, st), "color")) err = 1;
+  if (!err && bad(s->d_chunk.upload(L.chunk, st), "chunk")) err = 1;
+  if (!err && bad(s->d_rec_idx.upload(L.rec_idx, st), "rec_idx")) err = 1;
+  if (!err) {
+    // record values in the solver precision
+    const size_t nval = L.rec_val.size();
+    if (s->fp64) {
+      if (bad(s->d_rec_val.alloc(nval * 8), "rec_val")) err = 1;
+      if (!err && nval &&
+          bad(cudaMemcpyAsync(s->d_rec_val.p, L.rec_val.data(), nval * 8, cudaMemcpyHostToDevice,
+                              st),
+              "rec_val copy"))
+        err = 1;
+    } else {
+      std::vector<float> f(nval);
+      for (size_t i = 0; i < nval; ++i) f[i] = (float)L.rec_val[i];
+      if (bad(s->d_rec_val.alloc(nval * 4), "rec_val")) err = 1;
+      if (!err && nval &&
+          bad(cudaMemcpyAsync(s->d_rec_val.p, f.data(), nval * 4, cudaMemcpyHostToDevice, st),
+              "rec_val copy"))
+        err = 1;
+      if (!err) cudaStreamSynchronize(st);  // f goes out of scope
+    }
+  }
+  if (!err && bad(s->d_valence.upload(L.valence, st), "valence")) err = 1;
+  if (!err && bad(s->d_map.upload(L.new_of_old, st), "map")) err = 1;
+  std::vector<double> Xv(X, X + 3 * (size_t)V);
+  if (!err && bad(s->d_X.upload(Xv, st), "X")) err = 1;
+  if (!err && bad(s->d_io.alloc(3 * (size_t)V), "io")) err = 1;
+  if (!err && bad(s->d_tol.alloc(s->n_env), "tol")) err = 1;
+  if (!err && bad(s->d_iters.alloc(s->n_env), "iters")) err = 1;
+  if (!err && bad(s->d_status.alloc(s->n_env), "status")) err = 1;
+  if (!err && bad(s->d_params.alloc(1), "params")) err = 1;
+  if (!err && bad(s->d_ctl.alloc(1), "ctl")) err = 1;
+  const size_t sb = s->real4_bytes * (size_t)V;
+  for (auto* b : {&s->d_u, &s->d_ut, &s->d_up, &s->d_vel})
+    if (!err && bad(b->alloc(sb), "state")) err = 1;
+  if (!err) {
+    // state: u = up = vel = 0, ut.w = lumped mass
+    cudaMemsetAsync(s->d_u.p, 0, sb, st);
+    cudaMemsetAsync(s->d_up.p, 0, sb, st);
+    cudaMemsetAsync(s->d_vel.p, 0, sb, st);
+    if (s->state64) {
+      std::vector<double> ut(4 * (size_t)V, 0.0);
+      for (int i = 0; i < V; ++i) ut[4 * (size_t)i + 3] = L.mass[i];
+      if (bad(cudaMemcpyAsync(s->d_ut.p, ut.data(), sb, cudaMemcpyHostToDevice, st), "ut"))
+        err = 1;
+      cudaStreamSynchronize(st);
+    } else {
+      std::vector<float> ut(4 * (size_t)V, 0.0f);
+      for (int i = 0; i < V; ++i) ut[4 * (size_t)i + 3] = (float)L.mass[i];
+      if (bad(cudaMemcpyAsync(s->d_ut.p, ut.data(), sb, cudaMemcpyHostToDevice, st), "ut"))
+        err = 1;
+      cudaStreamSynchronize(st);
+    }
+    cudaMemsetAsync(s->d_iters.p, 0, sizeof(int) * s->n_env, st);
+    cudaMemsetAsync(s->d_status.p, 0, sizeof(unsigned) * s->n_env, st);
+  }
+  if (!err && bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_iters), sizeof(int) * s->n_env),
+                  "pinned"))
+    err = 1;
+  if (!err &&
+      bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_status), sizeof(unsigned) * s->n_env),
+          "pinned"))
+    err = 1;
+  if (!err && bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_params), sizeof(StepParams)),
+                  "pinned"))
+    err = 1;
+  if (!err && bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_ctl), sizeof(LoopControl)),
+                  "pinned"))
+    err = 1;
+  if (!err && bad(cudaStreamSynchronize(st), "setup sync")) err = 1;
+  if (err) {
+    free_solver(s);
+    return VBD_ERR_CUDA;
+  }
+  s->device_bytes = 0;
+  s->device_bytes += (long long)(s->d_rec_idx.n * sizeof(int4) + s->d_rec_val.n);
+  s->device_bytes += (long long)(4 * sb + s->d_X.n * 8 + s->d_io.n * 8);
+  s->device_bytes += (long long)(s->d_valence.n * 4 + s->d_map.n * 4);
+  *out = s;
+  return VBD_OK;
+}
+
+int status_from_bits(const vbd_solver* s, const unsigned* st) {
+  int rc = VBD_OK;
+  for (int e = 0; e < s->n_env; ++e) {
+    const unsigned b = st[e];
+    if (b & kStatNonFinite) return fail(VBD_ERR_NONFINITE, "non-finite value in the iterate");
+    if ((b & kStatGuard) && (s->flags & VBD_STRICT_SPD))
+      return fail(VBD_ERR_NONFINITE, "3x3 vertex block not positive definite");
+    if (b & kStatTimeout) return fail(VBD_ERR_TIMEOUT, "device-side wait timed out");
+    if (b & kStatIterCap) rc = VBD_NOT_CONVERGED;
+  }
+  return rc;
+}
+
+int set_params(vbd_solver* s, double dt, double tol, int max_iter) {
+  StepParams p{};
+  p.dt = dt;
+  p.tol = tol;
+  p.kd = s->kd;
+  p.g[0] = s->g[0];
+  p.g[1] = s->g[1];
+  p.g[2] = s->g[2];
+  p.max_iter = max_iter;
+  p.strict_spd = (s->flags & VBD_STRICT_SPD) ? 1 : 0;
+  if (s->params_valid && std::memcmp(&p, &s->cur_params, sizeof p) == 0) return VBD_OK;
+  // the pinned staging struct may still be read by an earlier copy
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  *s->h_params = p;
+  CUDA_TRY(cudaMemcpyAsync(s->d_params.p, s->h_params, sizeof p, cudaMemcpyHostToDevice,
+                           s->stream));
+  s->cur_params = p;
+  s->params_valid = true;
+  return VBD_OK;
+}
+
+int build_graph(vbd_solver* s) {
+  if (s->graph_exec) return VBD_OK;
+  cudaStream_t st = s->stream;
+  const DevMesh m = s->mesh();
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaGraphCreate(&g, 0));
+  s->graph = g;
+  CUDA_TRY(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+  cudaError_t le = launch_begin(s->state64, m, s->d_params.p, s->d_ctl.p, st);
+  cudaGraph_t gout = nullptr;
+  CUDA_TRY(cudaStreamEndCapture(st, &gout));
+  CUDA_TRY(le);
+  size_t n = 0;
+  CUDA_TRY(cudaGraphGetNodes(g, nullptr, &n));
+  if (n != 1) return fail(VBD_ERR_CUDA, "unexpected node count in the step graph");
+  cudaGraphNode_t begin_node;
+  CUDA_TRY(cudaGraphGetNodes(g, &begin_node, &n));
+  cudaGraphConditionalHandle handle;
+  CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, g, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cond_node;
+  CUDA_TRY(cudaGraphAddNode(&cond_node, g, &begin_node, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  CUDA_TRY(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+  le = cudaSuccess;
+  const EnvInfo& e = s->L.env[0];
+  for (int c = e.cbase; c < e.cbase + e.ncolors && le == cudaSuccess; ++c) {
+    const ColorInfo& ci = s->L.color[c];
+    le = launch_color(s->prec, s->material, s->tpv, s->threads, m, c,
+                      ci.chunk_end - ci.chunk_begin, s->d_params.p, s->d_ctl.p, st);
+  }
+  if (le == cudaSuccess)
+    le = launch_check(s->d_ctl.p, s->d_params.p, (unsigned long long)handle, 1, st);
+  CUDA_TRY(cudaStreamEndCapture(st, &gout));
+  CUDA_TRY(le);
+  CUDA_TRY(cudaStreamBeginCaptureToGraph(st, g, &cond_node, nullptr, 1,
+                                         cudaStreamCaptureModeThreadLocal));
+  le = launch_end(s->state64, m, s->d_params.p, s->d_ctl.p, st);
+  CUDA_TRY(cudaStreamEndCapture(st, &gout));
+  CUDA_TRY(le);
+  CUDA_TRY(cudaGraphInstantiate(&s->graph_exec, g, 0));
+  return VBD_OK;
+}
+
+int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, int max_iter) {
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(VBD_ERR_INVALID_ARG, "dt must be > 0");
+  if (max_iter < 1) return fail(VBD_ERR_INVALID_ARG, "max_iter must be >= 1");
+  int rc = set_params(s, dt, tol, max_iter);
+  if (rc != VBD_OK) return rc;
+  const DevMesh m = s->mesh();
+  cudaStream_t st = s->stream;
+  if (s->mode == VBD_MODE_BLOCK) {
+    const double* dtol = nullptr;
+    if (tol_env) {
+      CUDA_TRY(cudaStreamSynchronize(st));
+      CUDA_TRY(cudaMemcpy(s->d_tol.p, tol_env, sizeof(double) * s->n_env,
+                          cudaMemcpyHostToDevice));
+      dtol = s->d_tol.p;
+    }
+    CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
+                             s->n_env, s->smem_bytes, st));
+  } else if (s->mode == VBD_MODE_GRAPH) {
+    rc = build_graph(s);
+    if (rc != VBD_OK) return rc;
+    CUDA_TRY(cudaGraphLaunch(s->graph_exec, st));
+  } else {
+    // host-driven loop: one device->host read of the loop state per sweep
+    CUDA_TRY(launch_begin(s->state64, m, s->d_params.p, s->d_ctl.p, st));
+    const EnvInfo& e = s->L.env[0];
+    for (int it = 0; it < max_iter; ++it) {
+      for (int c = e.cbase; c < e.cbase + e.ncolors; ++c) {
+        const ColorInfo& ci = s->L.color[c];
+        CUDA_TRY(launch_color(s->prec, s->material, s->tpv, s->threads, m, c,
+                              ci.chunk_end - ci.chunk_begin, s->d_params.p, s->d_ctl.p, st));
+      }
+      CUDA_TRY(launch_check(s->d_ctl.p, s->d_params.p, 0ull, 0, st));
+      CUDA_TRY(cudaMemcpyAsync(s->h_ctl, s->d_ctl.p, sizeof(LoopControl), cudaMemcpyDeviceToHost,
+                               st));
+      CUDA_TRY(cudaStreamSynchronize(st));
+      if (s->h_ctl->status & 0x80000000u) break;
+    }
+    CUDA_TRY(launch_end(s->state64, m, s->d_params.p, s->d_ctl.p, st));
+  }
+  s->pending = true;
+  return VBD_OK;
+}
+
+int finish(vbd_solver* s, int* iters_out) {
+  cudaStream_t st = s->stream;
+  CUDA_TRY(cudaMemcpyAsync(s->h_iters, s->d_iters.p, sizeof(int) * s->n_env,
+                           cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(s->h_status, s->d_status.p, sizeof(unsigned) * s->n_env,
+                           cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  s->pending = false;
+  if (iters_out) std::memcpy(iters_out, s->h_iters, sizeof(int) * s->n_env);
+  s->last_status = status_from_bits(s, s->h_status);
+  return s->last_status;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int vbd_version(void) { return 1; }
+
+const char* vbd_status_string(int status) {
+  switch (status) {
+    case VBD_OK: return "ok";
+    case VBD_NOT_CONVERGED: return "not converged within max_iter";
+    case VBD_ERR_INVALID_ARG: return "invalid argument";
+    case VBD_ERR_CUDA: return "CUDA error";
+    case VBD_ERR_SINGULAR_DM: return "singular rest shape (zero-volume tet)";
+    case VBD_ERR_TOO_MANY_COLORS: return "colouring needs more than 256 colours";
+    case VBD_ERR_NONFINITE: return "non-finite value";
+    case VBD_ERR_TIMEOUT: return "device-side wait timed out";
+    case VBD_ERR_NO_DEVICE: return "no CUDA device";
+    case VBD_ERR_UNSUPPORTED: return "unsupported configuration";
+    default: return "unknown status";
+  }
+}
+
+const char* vbd_last_error_message(void) { return g_last_error.c_str(); }
+
+int vbd_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int vbd_graph_coloring(const int32_t* tets, int n_tets, int32_t* coloring_out,
+                       int* n_vertices_out, int* n_colors_out) {
+  if (n_tets < 0 || (n_tets > 0 && (!tets || !coloring_out)))
+    return fail(VBD_ERR_INVALID_ARG, "bad arguments");
+  int nv = 0;
+  for (size_t i = 0; i < 4 * (size_t)n_tets; ++i) {
+    if (tets[i] < 0) return fail(VBD_ERR_INVALID_ARG, "negative vertex id");
+    nv = std::max(nv, tets[i] + 1);
+  }
+  int nc = nv ? greedy_coloring(tets, n_tets, nv, coloring_out) : 0;
+  if (n_vertices_out) *n_vertices_out = nv;
+  if (nc < 0) return fail(VBD_ERR_TOO_MANY_COLORS, "Exceeded maximum number of colors");
+  if (n_colors_out) *n_colors_out = nc;
+  return VBD_OK;
+}
+
+int vbd_create(const double* rest_positions, int n_vertices, const int32_t* tets, int n_tets,
+               const double* densities, const double* youngs_modulus,
+               const double* poissons_ratio, const uint8_t* active_mask,
+               double damping_coefficient, const double* gravity, const int32_t* coloring,
+               int flags, int tpv, int block_threads, int device, vbd_solver** out) {
+  std::vector<int> voff{0, n_vertices}, toff{0, n_tets};
+  return create_impl(rest_positions, n_vertices, tets, n_tets, densities, youngs_modulus,
+                     poissons_ratio, active_mask, damping_coefficient, gravity, coloring, voff,
+                     toff, flags, tpv, block_threads, device, out);
+}
+
+int vbd_create_batched(const double* rest_positions, int n_vertices, const int32_t* tets,
+                       int n_tets, const double* densities, const double* youngs_modulus,
+                       const double* poissons_ratio, const uint8_t* active_mask,
+                       double damping_coefficient, const double* gravity,
+                       const int32_t* env_vertex_offset, const int32_t* env_tet_offset,
+                       int n_env, int flags, int tpv, int block_threads, int device,
+                       vbd_solver** out) {
+  if (n_env < 1 || !env_vertex_offset || !env_tet_offset)
+    return fail(VBD_ERR_INVALID_ARG, "n_env < 1 or NULL offsets");
+  if (env_vertex_offset[0] != 0 || env_tet_offset[0] != 0 ||
+      env_vertex_offset[n_env] != n_vertices || env_tet_offset[n_env] != n_tets)
+    return fail(VBD_ERR_INVALID_ARG, "environment offsets must span [0, n) exactly");
+  std::vector<int> voff(env_vertex_offset, env_vertex_offset + n_env + 1);
+  std::vector<int> toff(env_tet_offset, env_tet_offset + n_env + 1);
+  for (int e = 0; e < n_env; ++e)
+    if (voff[e + 1] <= voff[e] || toff[e + 1] < toff[e])
+      return fail(VBD_ERR_INVALID_ARG, "every environment needs >= 1 vertex");
+  return create_impl(rest_positions, n_vertices, tets, n_tets, densities, youngs_modulus,
+                     poissons_ratio, active_mask, damping_coefficient, gravity, nullptr, voff,
+                     toff, flags, tpv, block_threads, device, out);
+}
+
+void vbd_destroy(vbd_solver* s) { free_solver(s); }
+
+int vbd_reset(vbd_solver* s) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  DeviceGuard dg(s->device);
+  const size_t sb = s->real4_bytes * (size_t)s->V;
+  CUDA_TRY(cudaMemsetAsync(s->d_u.p, 0, sb, s->stream));
+  CUDA_TRY(cudaMemsetAsync(s->d_vel.p, 0, sb, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return VBD_OK;
+}
+
+int vbd_step(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  DeviceGuard dg(s->device);
+  int rc = enqueue_step(s, dt, tol, nullptr, max_iter);
+  if (rc != VBD_OK) return rc;
+  if (!iterations_out) return VBD_OK;
+  return finish(s, iterations_out);
+}
+
+int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per_env,
+                     int max_iter, int* iterations_out) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  DeviceGuard dg(s->device);
+  if (tol_per_env && s->mode != VBD_MODE_BLOCK)
+    return fail(VBD_ERR_UNSUPPORTED, "per-environment tolerances need block mode");
+  int rc = enqueue_step(s, dt, tol, tol_per_env, max_iter);
+  if (rc != VBD_OK) return rc;
+  if (!iterations_out) return VBD_OK;
+  return finish(s, iterations_out);
+}
+
+int vbd_sync(vbd_solver* s) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  DeviceGuard dg(s->device);
+  if (!s->pending) {
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return s->last_status;
+  }
+  return finish(s, nullptr);
+}
+
+int vbd_get_iterations(vbd_solver* s, int* iterations_out) {
+  if (!s || !iterations_out) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  DeviceGuard dg(s->device);
+  if (s->pending) {
+    int rc = finish(s, iterations_out);
+    return rc < 0 ? rc : VBD_OK;
+  }
+  std::memcpy(iterations_out, s->h_iters, sizeof(int) * s->n_env);
+  return VBD_OK;
+}
+
+static int exchange(vbd_solver* s, const double* in, double* out, bool positions) {
+  if (!s || (!in && !out)) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  DeviceGuard dg(s->device);
+  cudaStream_t st = s->stream;
+  const size_t bytes = sizeof(double) * 3 * (size_t)s->V;
+  void* state = positions ? (void*)s->d_u.p : (void*)s->d_vel.p;
+  const double* off = positions ? s->d_X.p : nullptr;
+  if (out) {
+    CUDA_TRY(launch_gather(s->state64, off, s->d_map.p, state, s->d_io.p, s->V, st));
+    CUDA_TRY(cudaMemcpyAsync(out, s->d_io.p, bytes, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+  } else {
+    CUDA_TRY(cudaStreamSynchronize(st));  // d_io may be in use by a pending gather
+    CUDA_TRY(cudaMemcpyAsync(s->d_io.p, in, bytes, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(launch_scatter(s->state64, off, s->d_map.p, s->d_io.p, state, s->V, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  return VBD_OK;
+}
+
+int vbd_get_positions(vbd_solver* s, double* x) { return exchange(s, nullptr, x, true); }
+int vbd_set_positions(vbd_solver* s, const double* x) { return exchange(s, x, nullptr, true); }
+int vbd_get_velocities(vbd_solver* s, double* v) { return exchange(s, nullptr, v, false); }
+int vbd_set_velocities(vbd_solver* s, const double* v) { return exchange(s, v, nullptr, false); }
+
+int vbd_get_color_groups(vbd_solver* s, int32_t* table, int* n_colors, int* max_group) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  if (n_colors) *n_colors = s->L.table_colors;
+  if (max_group) *max_group = s->L.table_max_group;
+  if (table && !s->L.table0.empty())
+    std::memcpy(table, s->L.table0.data(), sizeof(int32_t) * s->L.table0.size());
+  return VBD_OK;
+}
+
+int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
+  if (!s || !info) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  info->n_vertices = s->V;
+  info->n_tets = s->T;
+  info->n_env = s->n_env;
+  info->n_colors = s->L.max_colors;
+  info->max_valence = s->L.max_valence;
+  info->mode = s->mode;
+  info->tpv = s->tpv;
+  info->block_threads = s->threads;
+  info->precision = s->prec;
+  info->material = s->material;
+  info->n_slots = s->L.n_slots;
+  info->n_slot_records = s->n_records;
+  info->device_bytes = s->device_bytes;
+  return VBD_OK;
+}
+
+void* vbd_get_stream(vbd_solver* s) { return s ? (void*)s->stream : nullptr; }
+
+}  // extern "C"

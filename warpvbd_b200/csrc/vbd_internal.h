@@ -1,0 +1,92 @@
+// Internal layout shared by the host setup (vbd_host.cu) and the kernels
+// (vbd_kernels.cu).
+//
+// Device data of one solver ("mesh" = one or more independent environments):
+//
+//   vertices   renumbered so that, inside each environment, the solved
+//              vertices of colour 0, 1, ... are contiguous (sorted by valence
+//              inside a colour), followed by the "free" active vertices (not
+//              coloured or without incident tets: they follow the inertia
+//              guess) and then the fixed vertices.
+//   u, ut, up, vel   Real4 per vertex: displacement from the rest position,
+//              inertia target (w = lumped mass), displacement at step start,
+//              velocity.
+//   slots      one record per incident (vertex, tet) pair, SELL-32 layout: a
+//              "chunk" is 32 lanes = 32/TPV vertices x TPV lanes; chunk q has
+//              `steps` blocks of 32 records, block b holds, for lane l, slot
+//              j = s*TPV + (l % TPV) of vertex l / TPV.
+//              idx plane  int4  (n0, n1, n2, -)    environment-local ids of
+//                                                  the tet's other vertices
+//              val planes Real4 (b_n0, p0) (b_n1, p1) (b_n2, p2)
+//              b_n = gradient of the tet's linear shape function of vertex n
+//              (a row of Dm^-1, or minus their sum), p0 = V*mu, p1 = V*lambda
+//              (material-adjusted), p2 = alpha (SNH) or 0.
+#pragma once
+#include <cstdint>
+
+namespace vbd {
+
+enum Material : int { kSNH = 0, kStVK = 1 };
+
+// status bits written by the kernels (per environment)
+enum StatusBits : unsigned {
+  kStatNonFinite = 1u,
+  kStatGuard = 2u,      // a 3x3 block was not positive definite
+  kStatIterCap = 4u,    // max_iter reached without convergence
+  kStatTimeout = 8u,
+};
+
+struct EnvInfo {
+  int vbase;    // first (global, renumbered) vertex id
+  int nv;       // vertices
+  int nact;     // active vertices (solved + free) = local ids [0, nact)
+  int nsolved;  // solved vertices = local ids [0, nsolved)
+  int cbase;    // first colour record in the colour table
+  int ncolors;
+  int pad0, pad1;
+};
+
+struct ColorInfo {
+  int vbegin, vend;       // global vertex ids
+  int chunk_begin, chunk_end;
+};
+
+struct ChunkInfo {
+  int block;  // first 32-record block
+  int steps;  // number of blocks
+};
+
+struct StepParams {
+  double dt, tol, kd;
+  double g[3];
+  int max_iter;
+  int strict_spd;
+};
+
+// Grid-mode loop control (one per solver).
+struct LoopControl {
+  unsigned long long conv_bits;  // max |dx_x+dx_y+dx_z| of the current sweep, as
+                                 // the bits of a non-negative double (ordered
+                                 // like the values; NaN above +Inf)
+  int iter;                      // sweeps done in this step
+  unsigned status;
+};
+
+struct DevMesh {
+  const EnvInfo* env;
+  const ColorInfo* color;
+  const ChunkInfo* chunk;
+  const int4* rec_idx;
+  const void* rec_val;  // Real4
+  const int* valence;   // per global vertex
+  void* u;              // Real4
+  void* ut;
+  void* up;
+  void* vel;
+  int* iters;           // per env
+  unsigned* status;     // per env
+  int n_env;
+  int n_vertices;
+};
+
+}  // namespace vbd
