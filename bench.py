@@ -1,18 +1,23 @@
 """Benchmark of the VBD time step on B200.
 
-Default workload: the 160x16x16 Stable Neo-Hookean cantilever (1.0 x 0.1 x
-0.1 m beam, 46,529 vertices, 204,800 tets; E=1e6 Pa, nu=0.45, rho=1000, x=0
-face fixed, gravity -z, dt=1 ms, tol 1e-7, max 1000 sweeps), plain VBD in
-fp32.  A "step" is one implicit-Euler time step (inertia guess, colour sweeps
-until max|dx_x+dx_y+dx_z| < tol, velocity update).  value = simulated
-seconds per wall second, summed over ranks (each rank runs its own replica:
-weak scaling, no collective on the data path).
+Default workload (``--workload batch256``): 256 mass-spring environments of
+uneven size drawn from seed 0 (cube edge 7-15 voxels, column 5-30 voxels,
+1 cm voxels, E log-uniform 1e5-1e6 Pa, nu 0.35-0.48, rho 1000, the column's
+top face fixed, gravity -z), Stable Neo-Hookean, dt = 1 ms, tol 1e-7, at most
+1000 sweeps per step; fp32 arithmetic with fp64 positions.  All environments
+advance in one launch per step, each with its own convergence test.
+
+A "step" is one implicit-Euler time step of every environment (inertia guess,
+colour sweeps until max|dx_x+dx_y+dx_z| < tol, velocity update).
+value = simulated environment-seconds per wall second, summed over ranks
+(each rank steps its own copy of the batch: weak scaling, no collective on
+the data path).  Other workloads: cantilever20/40/80/160/320, massspring.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
-  python bench.py --impl reference ...   # the FP64 CPU oracle on the host cores
+  python bench.py --impl reference ...   # FP64 CPU oracle on the host cores
 
-Timing: every timed step is bracketed by CUDA events on the solver's stream,
-with a 256 MiB write between steps to flush L2; the e2e figure runs the same
+Timing: each timed step is bracketed by CUDA events on the solver's stream;
+a 256 MiB buffer is written between steps to flush L2.  The e2e figure runs
 steps through the public Python API with host arrays (positions uploaded
 before and downloaded after every step).
 """
@@ -35,44 +40,40 @@ TOL = 1e-7
 MAX_ITER = 1000
 
 
-def workload(name):
-    if name == "cantilever160":
-        return scenes.cantilever(160), "cantilever 160x16x16 SNH fp32"
-    if name == "cantilever80":
-        return scenes.cantilever(80), "cantilever 80x8x8 SNH fp32"
-    if name == "cantilever320":
-        return scenes.cantilever(320), "cantilever 320x32x32 SNH fp32"
-    if name == "cantilever20":
-        return scenes.cantilever(20), "cantilever 20x2x2 SNH fp32"
+def make_workload(name):
+    """-> (list of Scene environments, description, batched?)"""
+    if name == "batch256":
+        return (scenes.env_batch(256, seed=0),
+                "256 uneven mass-spring envs (seed 0), SNH, fp32 math / fp64 state", True)
+    if name.startswith("cantilever"):
+        n = int(name[len("cantilever"):])
+        return [scenes.cantilever(n)], f"cantilever {n}x{n // 10}x{n // 10} SNH, fp32 math / fp64 state", False
     if name == "massspring":
-        return scenes.mass_spring(11, 20), "mass-spring 11^3 cube + 1x1x20 column SNH fp32"
+        return [scenes.mass_spring(11, 20)], "mass-spring 11^3 cube + 1x1x20 column SNH", False
     raise SystemExit(f"unknown workload {name}")
 
 
-def bytes_per_sweep(s):
-    """Algorithmic bytes of one sweep: sum over solved vertices of 44 + 104 k_v
-    (fp32 state 44 B per vertex, 104 B per incident tet)."""
+def sweep_bytes(s):
+    """Algorithmic bytes of one sweep of one mesh: sum over solved vertices of
+    44 + 104 k_v (44 B of per-vertex state, 104 B per incident tet)."""
     k = np.bincount(s.tets.reshape(-1), minlength=s.n_vertices)
     solved = s.active & (k > 0)
-    return float((44 + 104 * k[solved]).sum()), int(solved.sum())
+    return float((44 + 104 * k[solved]).sum()), int(solved.sum()), int(k[solved].sum())
 
 
 def clocks_start():
     try:
-        f = open(os.path.join(ROOT, "gpurun_out", "clocks_bench.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else os.devnull, "w")
-        p = subprocess.Popen(
+        return subprocess.Popen(
             ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        return p, f
     except Exception:
-        return None, None
+        return None
 
 
-def clocks_stop(p, f, gpu_index):
+def clocks_stop(p, gpu_index):
     if p is None:
         return None
     p.terminate()
@@ -80,10 +81,7 @@ def clocks_stop(p, f, gpu_index):
         out, _ = p.communicate(timeout=5)
     except Exception:
         p.kill()
-        out = ""
-    if f:
-        f.write(out)
-        f.close()
+        return None
     sm, mx, reasons = [], [], set()
     names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
     for line in out.strip().splitlines():
@@ -107,28 +105,60 @@ def clocks_stop(p, f, gpu_index):
 def measured_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+            return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
 
 
-def cpu_baseline(s, steps_budget_s=20.0, max_steps=50):
-    """Time the FP64 oracle (OpenMP, all host threads) on whole steps of the
-    same workload; returns sim-s/wall-s and the sample description."""
+def profile_traffic_per_slot(kernel, workload):
+    """DRAM bytes per (vertex, tet) slot visit that ncu measured for `kernel`
+    on `workload` (summary committed under profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.{workload}.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_slot_visit:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def concat(envs):
+    """Concatenate environments into one mesh: the reference's own way of
+    batching (examples/run_mass_spring_parallel.py:40-58)."""
+    X, T, rho, E, nu, act = [], [], [], [], [], []
+    off = 0
+    for e in envs:
+        X.append(e.vertices)
+        T.append(e.tets + off)
+        rho.append(e.density)
+        E.append(e.youngs)
+        nu.append(e.poisson)
+        act.append(e.active)
+        off += e.n_vertices
+    return dict(initial_positions=np.concatenate(X), elements=np.concatenate(T),
+                densities=np.concatenate(rho), youngs_modulus=np.concatenate(E),
+                poissons_ratio=np.concatenate(nu), active_mask=np.concatenate(act))
+
+
+def oracle_rate(envs, budget_s, max_steps, warmup=0):
+    """The FP64 oracle (OpenMP on all host threads) stepping `envs` as one
+    concatenated mesh, as the reference batches; returns (env-sim-s per wall-s,
+    steps, threads)."""
     from oracle import oracle
     n = oracle.max_threads()
     oracle.set_threads(n)
-    o = oracle.OracleSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL,
+    o = oracle.OracleSolver(**concat(envs), damping_coefficient=0.0, dx_tol=TOL,
                             max_iter=MAX_ITER, guarded=True)
+    for _ in range(warmup):
+        o.step(None, DT)
     t0 = time.perf_counter()
     k = 0
-    while k < max_steps and (time.perf_counter() - t0) < steps_budget_s:
+    while k < max_steps and (k == 0 or time.perf_counter() - t0 < budget_s):
         o.step(None, DT)
         k += 1
     el = time.perf_counter() - t0
-    return {"value": k * DT / el, "unit": "sim-s/wall-s", "cores": n, "kind": "port",
-            "sample": f"first {k} steps of the same workload, FP64 C oracle, OpenMP {n} threads"}
+    return len(envs) * k * DT / el, k, n, el
 
 
 def dist_init():
@@ -136,127 +166,178 @@ def dist_init():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        import torch.distributed as dist
         import datetime
-        backend = "nccl"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
-def run_reference(args, s, desc):
+def cpu_sample(envs, batched):
+    return envs[:8] if batched else envs[:1]
+
+
+def run_reference(args, envs, desc, batched):
     world, rank, _ = dist_init()
     if rank != 0:
         return
-    from oracle import oracle
-    n = oracle.max_threads()
-    oracle.set_threads(n)
-    o = oracle.OracleSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL,
-                            max_iter=MAX_ITER, guarded=True)
-    budget = args.reference_budget_s
-    for _ in range(args.warmup):
-        o.step(None, DT)
-    t0 = time.perf_counter()
-    k = 0
-    while k < args.steps and (time.perf_counter() - t0) < budget:
-        o.step(None, DT)
-        k += 1
-    el = time.perf_counter() - t0
-    v = k * DT / el
+    sample = cpu_sample(envs, batched)
+    v, k, n, el = oracle_rate(sample, args.reference_budget_s, args.steps, warmup=0)
+    what = (f"{len(sample)} of the {len(envs)} environments concatenated into one mesh "
+            "(the reference's batching, one global convergence test)") if batched else \
+        "the whole mesh"
     line = {"impl": "reference", "metric": "sim-s/wall-s", "value": v, "unit": "sim-s/wall-s",
-            "n_gpus": args.gpus, "steps": k, "warmup": args.warmup,
-            "ms_per_step": 1e3 * el / k, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "dt": DT, "tol": TOL, "max_iter": MAX_ITER,
-                       "vertices": s.n_vertices, "tets": s.n_tets},
+            "n_gpus": args.gpus, "steps": k, "warmup": 0, "ms_per_step": 1e3 * el / k,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": desc, "dt": DT, "tol": TOL, "max_iter": MAX_ITER},
             "cpu_baseline": {"value": v, "unit": "sim-s/wall-s", "cores": n, "kind": "port",
-                             "sample": f"{k} whole steps after {args.warmup} warm-up steps "
-                                       "(FP64 C restatement of the reference; Warp is not "
-                                       "installable offline)"},
+                             "sample": f"{k} whole steps of {what}; FP64 C restatement of the "
+                                       "reference solver (warp-lang is not installable offline)"},
             "e2e": {"value": v, "unit": "sim-s/wall-s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, s, desc):
+def make_solver(envs, batched, local, mode="auto"):
+    if batched:
+        from warpvbd_b200 import BatchedVBDSolver
+        return BatchedVBDSolver(envs, dx_tol=TOL, max_iter=MAX_ITER, device=f"cuda:{local}")
+    from warpvbd_b200 import VBDSolver
+    s = envs[0]
+    return VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL, max_iter=MAX_ITER,
+                     device=f"cuda:{local}", mode=mode)
+
+
+def step_async(sol, batched):
+    if batched:
+        sol.step(DT, blocking=False)
+    else:
+        sol.step(sol.old_positions, DT, blocking=False)
+
+
+def timed_steps(sol, batched, steps, warmup, local, flush, sample_clocks=False):
+    """Per-step CUDA-event times (ms) and per-step sweep counts."""
+    import torch
+    stream = torch.cuda.ExternalStream(sol.stream, device=local)
+    for _ in range(warmup):
+        step_async(sol, batched)
+        sol.sync()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    iters = []
+    torch.cuda.synchronize()
+    clk = clocks_start() if sample_clocks else None
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(k & 0xFF)
+        evs[k][0].record(stream)
+        step_async(sol, batched)
+        evs[k][1].record(stream)
+        iters.append(np.array(sol.sync(), dtype=np.int64).reshape(-1))
+    torch.cuda.synchronize()
+    clocks = clocks_stop(clk, local) if sample_clocks else None
+    ms = np.array([a.elapsed_time(b) for a, b in evs])
+    return ms, np.stack(iters), clocks
+
+
+def run_ours(args, envs, desc, batched):
     import torch
     world, rank, local = dist_init()
     torch.cuda.set_device(local)
-    from warpvbd_b200 import VBDSolver
-    sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL, max_iter=MAX_ITER,
-                    device=f"cuda:{local}", mode=args.mode)
-    info = sol.info()
-    stream = torch.cuda.ExternalStream(sol.stream, device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-    # warm-up (graph instantiation happens here)
-    for _ in range(args.warmup):
-        sol.step(sol.old_positions, DT)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    iters = []
+    sol = make_solver(envs, batched, local, args.mode)
+    info = sol.info()
     if world > 1:
         torch.distributed.barrier()
-    torch.cuda.synchronize()
-    clk, clkf = clocks_start()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(k & 0xFF)
-            evs[k][0].record(stream)
-        sol.step(sol.old_positions, DT, blocking=False)
-        evs[k][1].record(stream)
-        iters.append(None)
-        sol.sync()
-        iters[-1] = sol.last_iterations
-    torch.cuda.synchronize()
-    clocks = clocks_stop(clk, clkf, local)
-    step_ms = np.array([a.elapsed_time(b) for a, b in evs])
-    total_ms = float(step_ms.sum())
+    ms, iters, clocks = timed_steps(sol, batched, args.steps, args.warmup, local, flush,
+                                    sample_clocks=True)
+    total_ms = float(ms.sum())
     if world > 1:
         t = torch.tensor([total_ms], device=f"cuda:{local}")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-    iters = np.array(iters)
-    value = world * args.steps * DT / (total_ms * 1e-3)
+    n_env = len(envs)
+    value = world * n_env * args.steps * DT / (total_ms * 1e-3)
 
-    # end to end through the public API with host arrays
-    x_host = sol.old_positions.numpy()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        x_host = sol.step(x_host, DT).numpy()
-    e2e_s = time.perf_counter() - t0
-    e2e = world * args.e2e_steps * DT / e2e_s
-
-    bsweep, nsolved = bytes_per_sweep(s)
-    peak, peak_kind = measured_peak()
-    mode = {0x100: "block", 0x200: "graph", 0x300: "hostloop"}[info["mode"]]
-    achieved = bsweep * iters.sum() / (total_ms * 1e-3) / 1e9
-    if mode == "block":
-        launches = args.steps
+    # end to end through the public API, host arrays in and out every step
+    n_vertices = sum(e.n_vertices for e in envs)
+    if batched:
+        x = sol.positions()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            sol.set_state(positions=x)
+            sol.step(DT)
+            x = sol.positions()
+        e2e_s = time.perf_counter() - t0
     else:
-        launches = int(args.steps * 2 + iters.sum() * (info["n_colors"] + 1))
+        x = sol.old_positions.numpy()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            x = sol.step(x, DT).numpy()
+        e2e_s = time.perf_counter() - t0
+    e2e = world * n_env * args.e2e_steps * DT / e2e_s
+
+    # roofline of the dominant kernel: algorithmic bytes of the sweeps it ran
+    per_env = [sweep_bytes(e) for e in envs]
+    b_sweep = np.array([p[0] for p in per_env])
+    slots = np.array([p[2] for p in per_env])
+    solved = np.array([p[1] for p in per_env])
+    mode = {0x100: "block", 0x200: "graph", 0x300: "hostloop"}[info["mode"]]
+    alg_bytes = float((iters * b_sweep[None, :]).sum())
+    achieved = alg_bytes / (total_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    kernel = "env_step_kernel" if mode == "block" else "color_kernel"
+    tps = profile_traffic_per_slot(kernel, args.workload)
+    traffic = None if tps is None else tps * float((iters * slots[None, :]).sum()) / args.steps
+    launches = args.steps if mode == "block" else int(
+        args.steps * 2 + iters.sum() * (info["n_colors"] + 1))
     line = {"metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "dt": DT, "tol": TOL, "max_iter": MAX_ITER,
-                       "vertices": s.n_vertices, "tets": s.n_tets, "mode": mode,
-                       "tpv": info["tpv"], "block_threads": info["block_threads"],
+            "config": {"workload": desc, "n_env": n_env, "vertices": n_vertices,
+                       "tets": int(sum(e.n_tets for e in envs)), "dt": DT, "tol": TOL,
+                       "max_iter": MAX_ITER, "mode": mode, "tpv": info["tpv"],
+                       "block_threads": info["block_threads"],
                        "parallelism": f"replicas x{world}",
-                       "l2": "256 MiB buffer written between timed steps"},
-            "iters_per_step": {"mean": float(iters.mean()), "min": int(iters.min()),
-                               "max": int(iters.max())},
-            "vertex_updates_per_s": world * nsolved * float(iters.sum()) / (total_ms * 1e-3),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "peak_source": peak_kind,
-                         "algorithmic_bytes_per_sweep": bsweep},
+                       "l2": "256 MiB written between timed steps"},
+            "iters_per_step": {"mean": float(iters.mean()), "max": int(iters.max()),
+                               "min": int(iters.min())},
+            "vertex_updates_per_s": world * float((iters * solved[None, :]).sum())
+            / (total_ms * 1e-3),
+            "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes / args.steps},
             "e2e": {"value": e2e, "unit": "sim-s/wall-s",
-                    "h2d_bytes_per_step": 24 * s.n_vertices,
-                    "d2h_bytes_per_step": 24 * s.n_vertices},
+                    "h2d_bytes_per_step": 24 * n_vertices,
+                    "d2h_bytes_per_step": 24 * n_vertices},
             "gpu_launches": launches}
     if clocks:
         line["clocks"] = clocks
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(s, args.cpu_budget_s)
+        sample = cpu_sample(envs, batched)
+        v, k, n, el = oracle_rate(sample, args.cpu_budget_s, 50)
+        line["cpu_baseline"] = {
+            "value": v, "unit": "sim-s/wall-s", "cores": n, "kind": "port",
+            "sample": f"{k} whole steps of {len(sample)} environment(s) "
+                      + ("concatenated into one mesh " if batched else "")
+                      + f"({el:.1f} s), FP64 C oracle, OpenMP {n} threads"}
+    if rank == 0 and world == 1 and batched and not args.no_secondary:
+        # the plain single-mesh solver on the 160x16x16 cantilever
+        cant = scenes.cantilever(160)
+        cs = make_solver([cant], False, local)
+        cms, cit, _ = timed_steps(cs, False, args.secondary_steps, 3, local, flush)
+        cb, csolved, _ = sweep_bytes(cant)
+        t = float(cms.sum()) * 1e-3
+        line["cantilever160"] = {
+            "sim_s_per_wall_s": args.secondary_steps * DT / t,
+            "ms_per_step": 1e3 * t / args.secondary_steps,
+            "iters_per_step": float(cit.mean()), "mode": {0x100: "block", 0x200: "graph"}.get(
+                cs.info()["mode"], "hostloop"),
+            "vertex_updates_per_s": csolved * float(cit.sum()) / t,
+            "roofline_frac": cb * float(cit.sum()) / t / 1e9 / peak}
+        cs.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -267,22 +348,24 @@ def run_ours(args, s, desc):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cantilever160")
+    ap.add_argument("--workload", default="batch256")
     ap.add_argument("--mode", default="auto", choices=["auto", "block", "graph", "hostloop"])
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--secondary-steps", type=int, default=30)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
-    ap.add_argument("--reference-budget-s", type=float, default=150.0)
+    ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    s, desc = workload(args.workload)
+    envs, desc, batched = make_workload(args.workload)
     if args.impl == "reference":
-        run_reference(args, s, desc)
+        run_reference(args, envs, desc, batched)
     else:
-        run_ours(args, s, desc)
+        run_ours(args, envs, desc, batched)
 
 
 if __name__ == "__main__":

@@ -156,6 +156,7 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info);
 /* The CUDA stream (cudaStream_t) all of the solver's work is enqueued on. */
 void* vbd_get_stream(vbd_solver* s);
 
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,350 @@
+// Device-side building blocks shared by the solver kernels (vbd_kernels.cu)
+// and the allocation-free step (vbd_noalloc.cu): vector types, the per-slot
+// elastic terms, the guarded 3x3 solve and the per-chunk vertex update.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "vbd_internal.h"
+
+namespace vbd {
+
+template <typename Real>
+struct V4;
+template <>
+struct V4<float> {
+  using type = float4;
+};
+template <>
+struct V4<double> {
+  using type = double4;
+};
+template <typename Real>
+using real4 = typename V4<Real>::type;
+
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ unsigned long long conv_bits(double c) {
+  // c >= 0 or NaN; fabs clears the sign so NaN bits sort above +Inf
+  return static_cast<unsigned long long>(__double_as_longlong(fabs(c)));
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    unsigned long long o = __shfl_xor_sync(0xffffffffu, v, off);
+    v = o > v ? o : v;
+  }
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Elastic gradient / Hessian of one (vertex, tet) slot, accumulated into g, h
+// (h = h00 h01 h02 h11 h12 h22).  d* = u_n - u_v of the tet's other three
+// vertices, q* = (b_n, p): p0 = V*mu, p1 = V*lambda (material-adjusted).
+// ---------------------------------------------------------------------------
+template <typename Real, int MAT>
+__device__ __forceinline__ void slot_accumulate(Real d0x, Real d0y, Real d0z, Real d1x, Real d1y,
+                                                Real d1z, Real d2x, Real d2y, Real d2z,
+                                                const real4<Real>& q0, const real4<Real>& q1,
+                                                const real4<Real>& q2, Real* g, Real* h) {
+  const Real G00 = d0x * q0.x + d1x * q1.x + d2x * q2.x;
+  const Real G01 = d0x * q0.y + d1x * q1.y + d2x * q2.y;
+  const Real G02 = d0x * q0.z + d1x * q1.z + d2x * q2.z;
+  const Real G10 = d0y * q0.x + d1y * q1.x + d2y * q2.x;
+  const Real G11 = d0y * q0.y + d1y * q1.y + d2y * q2.y;
+  const Real G12 = d0y * q0.z + d1y * q1.z + d2y * q2.z;
+  const Real G20 = d0z * q0.x + d1z * q1.x + d2z * q2.x;
+  const Real G21 = d0z * q0.y + d1z * q1.y + d2z * q2.y;
+  const Real G22 = d0z * q0.z + d1z * q1.z + d2z * q2.z;
+  const Real bx = -(q0.x + q1.x + q2.x);
+  const Real by = -(q0.y + q1.y + q2.y);
+  const Real bz = -(q0.z + q1.z + q2.z);
+  const Real p0 = q0.w, p1 = q1.w;
+  const Real bb = bx * bx + by * by + bz * bz;
+  const Real Gbx = G00 * bx + G01 * by + G02 * bz;
+  const Real Gby = G10 * bx + G11 * by + G12 * bz;
+  const Real Gbz = G20 * bx + G21 * by + G22 * bz;
+  const Real Fbx = bx + Gbx, Fby = by + Gby, Fbz = bz + Gbz;
+  const Real t = G00 + G11 + G22;
+  if (MAT == kSNH) {
+    const Real c00 = G11 * G22 - G12 * G21, c01 = G12 * G20 - G10 * G22,
+               c02 = G10 * G21 - G11 * G20;
+    const Real c10 = G21 * G02 - G22 * G01, c11 = G22 * G00 - G20 * G02,
+               c12 = G20 * G01 - G21 * G00;
+    const Real c20 = G01 * G12 - G02 * G11, c21 = G02 * G10 - G00 * G12,
+               c22 = G00 * G11 - G01 * G10;
+    const Real detG = G00 * c00 + G01 * c01 + G02 * c02;
+    const Real trG2 =
+        G00 * G00 + G11 * G11 + G22 * G22 + Real(2) * (G01 * G10 + G02 * G20 + G12 * G21);
+    const Real nG2 = G00 * G00 + G01 * G01 + G02 * G02 + G10 * G10 + G11 * G11 + G12 * G12 +
+                     G20 * G20 + G21 * G21 + G22 * G22;
+    const Real Jm1 = t + Real(0.5) * (t * t - trG2) + detG;
+    const Real Icm3 = Real(2) * t + nG2;
+    const Real inv = Real(1) / (Icm3 + Real(4));
+    const Real GTbx = G00 * bx + G10 * by + G20 * bz;
+    const Real GTby = G01 * bx + G11 * by + G21 * bz;
+    const Real GTbz = G02 * bx + G12 * by + G22 * bz;
+    const Real cGbx = c00 * bx + c01 * by + c02 * bz;
+    const Real cGby = c10 * bx + c11 * by + c12 * bz;
+    const Real cGbz = c20 * bx + c21 * by + c22 * bz;
+    const Real t1 = Real(1) + t;
+    const Real Cbx = t1 * bx - GTbx + cGbx;
+    const Real Cby = t1 * by - GTby + cGby;
+    const Real Cbz = t1 * bz - GTbz + cGbz;
+    const Real a = Real(0.25) * p0 * Icm3 * inv;
+    const Real k3 = Real(0.75) * p0;
+    const Real kJ = p1 * Jm1;
+    g[0] += a * Fbx + k3 * (Gbx + GTbx - t * bx - cGbx) + kJ * Cbx;
+    g[1] += a * Fby + k3 * (Gby + GTby - t * by - cGby) + kJ * Cby;
+    g[2] += a * Fbz + k3 * (Gbz + GTbz - t * bz - cGbz) + kJ * Cbz;
+    const Real hF = Real(2) * p0 * inv * inv;
+    const Real hI = p0 * (Icm3 + Real(3)) * inv * bb;
+    const Real Fx = hF * Fbx, Fy = hF * Fby, Fz = hF * Fbz;
+    const Real Cx = p1 * Cbx, Cy = p1 * Cby, Cz = p1 * Cbz;
+    h[0] += Fx * Fbx + Cx * Cbx + hI;
+    h[1] += Fx * Fby + Cx * Cby;
+    h[2] += Fx * Fbz + Cx * Cbz;
+    h[3] += Fy * Fby + Cy * Cby + hI;
+    h[4] += Fy * Fbz + Cy * Cbz;
+    h[5] += Fz * Fbz + Cz * Cbz + hI;
+  } else {
+    // E = (G + G^T + G^T G) / 2
+    const Real E00 = G00 + Real(0.5) * (G00 * G00 + G10 * G10 + G20 * G20);
+    const Real E11 = G11 + Real(0.5) * (G01 * G01 + G11 * G11 + G21 * G21);
+    const Real E22 = G22 + Real(0.5) * (G02 * G02 + G12 * G12 + G22 * G22);
+    const Real E01 = Real(0.5) * (G01 + G10 + G00 * G01 + G10 * G11 + G20 * G21);
+    const Real E02 = Real(0.5) * (G02 + G20 + G00 * G02 + G10 * G12 + G20 * G22);
+    const Real E12 = Real(0.5) * (G12 + G21 + G01 * G02 + G11 * G12 + G21 * G22);
+    const Real trE = E00 + E11 + E22;
+    const Real Ebx = E00 * bx + E01 * by + E02 * bz;
+    const Real Eby = E01 * bx + E11 * by + E12 * bz;
+    const Real Ebz = E02 * bx + E12 * by + E22 * bz;
+    const Real FEbx = Ebx + G00 * Ebx + G01 * Eby + G02 * Ebz;
+    const Real FEby = Eby + G10 * Ebx + G11 * Eby + G12 * Ebz;
+    const Real FEbz = Ebz + G20 * Ebx + G21 * Eby + G22 * Ebz;
+    const Real k2 = Real(2) * p0, kt = p1 * trE;
+    g[0] += k2 * FEbx + kt * Fbx;
+    g[1] += k2 * FEby + kt * Fby;
+    g[2] += k2 * FEbz + kt * Fbz;
+    const Real bEb = bx * Ebx + by * Eby + bz * Ebz;
+    // F F^T = I + G + G^T + G G^T
+    const Real A00 = Real(1) + Real(2) * G00 + G00 * G00 + G01 * G01 + G02 * G02;
+    const Real A11 = Real(1) + Real(2) * G11 + G10 * G10 + G11 * G11 + G12 * G12;
+    const Real A22 = Real(1) + Real(2) * G22 + G20 * G20 + G21 * G21 + G22 * G22;
+    const Real A01 = G01 + G10 + G00 * G10 + G01 * G11 + G02 * G12;
+    const Real A02 = G02 + G20 + G00 * G20 + G01 * G21 + G02 * G22;
+    const Real A12 = G12 + G21 + G10 * G20 + G11 * G21 + G12 * G22;
+    const Real kff = p1 + p0;
+    const Real kA = p0 * bb;
+    const Real kI = kt * bb + k2 * bEb;
+    h[0] += kff * Fbx * Fbx + kA * A00 + kI;
+    h[1] += kff * Fbx * Fby + kA * A01;
+    h[2] += kff * Fbx * Fbz + kA * A02;
+    h[3] += kff * Fby * Fby + kA * A11 + kI;
+    h[4] += kff * Fby * Fbz + kA * A12;
+    h[5] += kff * Fbz * Fbz + kA * A22 + kI;
+  }
+}
+
+// Guarded Newton step: solve H dx = -g by 3x3 Cholesky (the reference's
+// tile_cholesky / tile_cholesky_solve, vbd_solver.py:267-268).  Returns false
+// when a pivot is not positive (H not positive definite).
+template <typename Real>
+__device__ __forceinline__ bool chol_solve3(const Real* h, const Real* g, Real* x) {
+  const Real L00 = sqrt(h[0]);
+  const Real i0 = Real(1) / L00;
+  const Real L10 = h[1] * i0, L20 = h[2] * i0;
+  const Real d1 = h[3] - L10 * L10;
+  const Real L11 = sqrt(d1);
+  const Real i1 = Real(1) / L11;
+  const Real L21 = (h[4] - L20 * L10) * i1;
+  const Real d2 = h[5] - L20 * L20 - L21 * L21;
+  const Real L22 = sqrt(d2);
+  const Real i2 = Real(1) / L22;
+  const Real y0 = -g[0] * i0;
+  const Real y1 = (-g[1] - L10 * y0) * i1;
+  const Real y2 = (-g[2] - L20 * y0 - L21 * y1) * i2;
+  x[2] = y2 * i2;
+  x[1] = (y1 - L21 * x[2]) * i1;
+  x[0] = (y0 - L10 * x[1] - L20 * x[2]) * i0;
+  return (h[0] > Real(0)) && (d1 > Real(0)) && (d2 > Real(0));
+}
+
+struct StepConst {
+  double inv_dt2, kd_dt, dt, dt2;
+  double g[3];
+  bool damp, strict;
+};
+
+__device__ __forceinline__ StepConst make_const(const StepParams& p) {
+  StepConst c;
+  c.dt = p.dt;
+  c.dt2 = p.dt * p.dt;
+  c.inv_dt2 = 1.0 / c.dt2;
+  c.kd_dt = p.kd / p.dt;
+  c.damp = p.kd != 0.0;
+  c.strict = p.strict_spd != 0;
+  c.g[0] = p.g[0];
+  c.g[1] = p.g[1];
+  c.g[2] = p.g[2];
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// One warp processes one chunk (32/TPV vertices of one colour).  `ul` indexes
+// the environment's displacements by environment-local id (shared memory in
+// block mode, global memory in grid mode).
+// ---------------------------------------------------------------------------
+template <typename Real, typename SReal, int TPV, int MAT, bool SMEM>
+__device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const ColorInfo& ci,
+                                              int q, int lane, real4<SReal>* ul,
+                                              const StepConst& sc, unsigned long long& cmax,
+                                              unsigned& stat) {
+  using R4 = real4<Real>;
+  using S4 = real4<SReal>;
+  constexpr int CPW = 32 / TPV;
+  const int vi = lane / TPV, sub = lane % TPV;
+  const int gv = ci.vbegin + (q - ci.chunk_begin) * CPW + vi;
+  const bool valid = gv < ci.vend;
+  const int lv = gv - vbase;
+  const ChunkInfo ch = m.chunk[q];
+  int k = 0;
+  S4 uo;
+  uo.x = uo.y = uo.z = uo.w = SReal(0);
+  if (valid) {
+    k = __ldg(m.valence + gv);
+    uo = SMEM ? ul[lv] : ldg4(ul + lv);
+  }
+  Real g[3] = {Real(0), Real(0), Real(0)};
+  Real h[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
+  const int4* ridx = m.rec_idx + (size_t)ch.block * 32 + lane;
+  const R4* rval = reinterpret_cast<const R4*>(m.rec_val) + (size_t)ch.block * 96 + lane;
+#pragma unroll 2
+  for (int s = 0; s < ch.steps; ++s) {
+    if (s * TPV + sub < k) {
+      const int4 id = __ldg(ridx + (size_t)s * 32);
+      const R4 q0 = ldg4(rval + (size_t)s * 96);
+      const R4 q1 = ldg4(rval + (size_t)s * 96 + 32);
+      const R4 q2 = ldg4(rval + (size_t)s * 96 + 64);
+      S4 a, b, c;
+      if (SMEM) {
+        a = ul[id.x];
+        b = ul[id.y];
+        c = ul[id.z];
+      } else {
+        a = ldg4(ul + id.x);
+        b = ldg4(ul + id.y);
+        c = ldg4(ul + id.z);
+      }
+      // neighbour offsets formed in the state precision, then rounded
+      slot_accumulate<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                                 Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                                 Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z), q0, q1,
+                                 q2, g, h);
+    }
+  }
+#pragma unroll
+  for (int off = TPV / 2; off > 0; off >>= 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) g[i] += __shfl_xor_sync(0xffffffffu, g[i], off);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) h[i] += __shfl_xor_sync(0xffffffffu, h[i], off);
+  }
+  if (valid && sub == 0) {
+    const S4 tt = ldg4(reinterpret_cast<const S4*>(m.ut) + gv);
+    const Real mdt2 = Real(tt.w * SReal(sc.inv_dt2));
+    Real G[3], H[6];
+    G[0] = g[0] + mdt2 * Real(uo.x - tt.x);
+    G[1] = g[1] + mdt2 * Real(uo.y - tt.y);
+    G[2] = g[2] + mdt2 * Real(uo.z - tt.z);
+    if (sc.damp) {
+      // Rayleigh-like damping kd * H_el (x - x_prev) / dt (vbd_solver.py:222-223)
+      const S4 u0 = ldg4(reinterpret_cast<const S4*>(m.up) + gv);
+      const Real kd = Real(sc.kd_dt);
+      const Real ex = Real(uo.x - u0.x), ey = Real(uo.y - u0.y), ez = Real(uo.z - u0.z);
+      G[0] += kd * (h[0] * ex + h[1] * ey + h[2] * ez);
+      G[1] += kd * (h[1] * ex + h[3] * ey + h[4] * ez);
+      G[2] += kd * (h[2] * ex + h[4] * ey + h[5] * ez);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) h[i] *= (Real(1) + kd);
+    }
+    H[0] = h[0] + mdt2;
+    H[1] = h[1];
+    H[2] = h[2];
+    H[3] = h[3] + mdt2;
+    H[4] = h[4];
+    H[5] = h[5] + mdt2;
+    Real dx[3];
+    if (!chol_solve3<Real>(H, G, dx)) {
+      stat |= kStatGuard;
+      if (!sc.strict) {
+        // fallback: inertia-only Hessian (m/dt^2) I; a massless vertex stays
+        const Real s = mdt2 > Real(0) ? Real(-1) / mdt2 : Real(0);
+        dx[0] = G[0] * s;
+        dx[1] = G[1] * s;
+        dx[2] = G[2] * s;
+      }
+    }
+    S4 un = uo;
+    un.x += SReal(dx[0]);
+    un.y += SReal(dx[1]);
+    un.z += SReal(dx[2]);
+    ul[lv] = un;
+    const double c = fabs(double(dx[0] + dx[1] + dx[2]));
+    if (!isfinite(c)) stat |= kStatNonFinite;
+    const unsigned long long cb = conv_bits(c);
+    cmax = cb > cmax ? cb : cmax;
+  }
+}
+
+// Inertia target and initial guess (position_initialization,
+// vbd_solver.py:277-292): ut = u + dt v + dt^2 g (w keeps the lumped mass),
+// up = u, and active vertices start from ut.
+template <typename Real>
+__device__ __forceinline__ real4<Real> begin_vertex(const DevMesh& m, int gv, bool active,
+                                                    const StepConst& sc) {
+  using R4 = real4<Real>;
+  R4* U = reinterpret_cast<R4*>(m.u);
+  R4* UT = reinterpret_cast<R4*>(m.ut);
+  R4* UP = reinterpret_cast<R4*>(m.up);
+  const R4* VEL = reinterpret_cast<const R4*>(m.vel);
+  const R4 u0 = U[gv];
+  const R4 v0 = VEL[gv];
+  R4 tt = UT[gv];
+  const Real dt = Real(sc.dt), dt2 = Real(sc.dt2);
+  tt.x = u0.x + v0.x * dt + Real(sc.g[0]) * dt2;
+  tt.y = u0.y + v0.y * dt + Real(sc.g[1]) * dt2;
+  tt.z = u0.z + v0.z * dt + Real(sc.g[2]) * dt2;
+  UT[gv] = tt;
+  UP[gv] = u0;
+  R4 un = u0;
+  if (active) {
+    un.x = tt.x;
+    un.y = tt.y;
+    un.z = tt.z;
+  }
+  return un;
+}
+
+// Velocity update (vbd_solver.py:609): v = (x_new - x_old) / dt.
+template <typename Real>
+__device__ __forceinline__ void end_vertex(const DevMesh& m, int gv, const real4<Real>& un,
+                                           const StepConst& sc) {
+  using R4 = real4<Real>;
+  const R4 u0 = reinterpret_cast<const R4*>(m.up)[gv];
+  R4 v;
+  const Real idt = Real(1.0 / sc.dt);
+  v.x = (un.x - u0.x) * idt;
+  v.y = (un.y - u0.y) * idt;
+  v.z = (un.z - u0.z) * idt;
+  v.w = Real(0);
+  reinterpret_cast<R4*>(m.vel)[gv] = v;
+}
+
+}  // namespace vbd
