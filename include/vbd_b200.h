@@ -156,6 +156,22 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info);
 /* The CUDA stream (cudaStream_t) all of the solver's work is enqueued on. */
 void* vbd_get_stream(vbd_solver* s);
 
+/* vbd_step for callers that may not allocate GPU memory while they step: an
+ * application that commits its whole device-memory budget at start-up, or a
+ * real-time loop whose per-step code may not call an allocator.  Create the
+ * solver once at start-up with vbd_create; this call then allocates nothing
+ * (no cudaMalloc / cudaFree, no graph instantiation) and blocks until the step
+ * is done.  It has no counterpart in the reference.
+ * The sweep's scratch (step parameters, loop control, one convergence partial
+ * per thread block) lives in one static device array of 131,200 bytes that
+ * every GPU loading the library holds until exit: a mesh whose sweep needs
+ * more than 16,384 thread blocks (a largest colour of about one million
+ * vertices at 4 lanes per vertex) is rejected with VBD_ERR_UNSUPPORTED, as
+ * is a batched solver.  All calls share the array: calls whose GPU work
+ * overlaps (other streams, other host threads) race and must be serialised.
+ * The first call on a device resolves the array's device address, so make it
+ * before any stream capture on that device. */
+int vbd_step_noalloc(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out);
 
 #ifdef __cplusplus
 }

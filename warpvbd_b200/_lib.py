@@ -85,6 +85,8 @@ SIGNATURES = {
     "vbd_get_color_groups": (ctypes.c_int, [_vp, _i, _ip, _ip]),
     "vbd_get_info": (ctypes.c_int, [_vp, ctypes.POINTER(VBDInfo)]),
     "vbd_get_stream": (_vp, [_vp]),
+    "vbd_step_noalloc": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                        _ip]),
 }
 
 _lib = None

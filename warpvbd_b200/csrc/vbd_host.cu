@@ -21,6 +21,7 @@
 #include "../../include/vbd_b200.h"
 #include "vbd_internal.h"
 #include "vbd_launch.h"
+#include "vbd_noalloc.h"
 
 using namespace vbd;
 
@@ -981,5 +982,67 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
 }
 
 void* vbd_get_stream(vbd_solver* s) { return s ? (void*)s->stream : nullptr; }
+
+// Allocation-free step (see vbd_noalloc.cu for who needs it and the limits of
+// its static scratch).  Runs the grid-mode colour sweep one sweep at a time
+// from the host; every buffer it touches either belongs to the solver (made
+// by vbd_create) or is the static scratch.
+int vbd_step_noalloc(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  if (s->n_env != 1)
+    return fail(VBD_ERR_UNSUPPORTED, "vbd_step_noalloc steps single-environment solvers");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(VBD_ERR_INVALID_ARG, "dt must be > 0");
+  if (max_iter < 1) return fail(VBD_ERR_INVALID_ARG, "max_iter must be >= 1");
+  DeviceGuard dg(s->device);
+  const EnvInfo& e = s->L.env[0];
+  int total = 0;  // convergence partials one sweep writes (one per thread block)
+  for (int c = e.cbase; c < e.cbase + e.ncolors; ++c) {
+    const ColorInfo& ci = s->L.color[c];
+    total += (ci.chunk_end - ci.chunk_begin + 7) / 8;
+  }
+  if (total > noalloc_max_partials())
+    return fail(VBD_ERR_UNSUPPORTED,
+                "vbd_step_noalloc: this mesh needs " + std::to_string(total) +
+                    " convergence partials per sweep; its static scratch holds " +
+                    std::to_string(noalloc_max_partials()));
+  unsigned long long* scratch = nullptr;
+  CUDA_TRY(noalloc_scratch_address(&scratch));
+  LoopControl* ctl = reinterpret_cast<LoopControl*>(scratch + kNoAllocCtlOffset);
+  StepParams* dp = reinterpret_cast<StepParams*>(scratch + kNoAllocParamOffset);
+  unsigned long long* partial = scratch + kNoAllocPartialOffset;
+  StepParams p{};
+  p.dt = dt;
+  p.tol = tol;
+  p.kd = s->kd;
+  p.g[0] = s->g[0];
+  p.g[1] = s->g[1];
+  p.g[2] = s->g[2];
+  p.max_iter = max_iter;
+  p.strict_spd = (s->flags & VBD_STRICT_SPD) ? 1 : 0;
+  cudaStream_t st = s->stream;
+  const DevMesh m = s->mesh();
+  // from pageable memory: the copy has read `p` when the call returns
+  CUDA_TRY(cudaMemcpyAsync(dp, &p, sizeof p, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(launch_begin(s->state64, m, dp, ctl, st));  // also zeroes the loop control
+  LoopControl hc{};
+  for (int it = 0; it < max_iter; ++it) {
+    int off = 0;
+    for (int c = e.cbase; c < e.cbase + e.ncolors; ++c) {
+      const ColorInfo& ci = s->L.color[c];
+      const int blocks = (ci.chunk_end - ci.chunk_begin + 7) / 8;
+      CUDA_TRY(launch_noalloc_color(s->prec, s->material, s->tpv, m, c, blocks, dp, ctl,
+                                    partial + off, st));
+      off += blocks;
+    }
+    CUDA_TRY(launch_noalloc_reduce(partial, off, ctl, st));
+    CUDA_TRY(launch_check(ctl, dp, 0ull, 0, st));
+    CUDA_TRY(cudaMemcpyAsync(&hc, ctl, sizeof hc, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (hc.status & 0x80000000u) break;
+  }
+  CUDA_TRY(launch_end(s->state64, m, dp, ctl, st));
+  s->pending = true;
+  return finish(s, iterations_out);
+}
 
 }  // extern "C"
