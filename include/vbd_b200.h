@@ -68,6 +68,11 @@ typedef struct vbd_solver vbd_solver;
 /* fail a step instead of taking the guarded fallback when a 3x3 block is not
  * positive definite (the reference would produce NaN there) */
 #define VBD_STRICT_SPD 0x2000
+/* block mode: thread blocks per cluster (1, 2, 4, 8, 16; 0 = automatic).  An
+ * environment much heavier than the others is split over all blocks of one
+ * cluster, which share its state through distributed shared memory. */
+#define VBD_CLUSTER_SHIFT 16
+#define VBD_CLUSTER(n) ((n) << VBD_CLUSTER_SHIFT)
 
 /* ---- library / device --------------------------------------------------- */
 int vbd_version(void);
@@ -91,7 +96,7 @@ int vbd_graph_coloring(const int32_t* tets, int n_tets, int32_t* coloring_out,
  *   damping_coefficient, gravity[3]
  *   coloring        int32   [max(tets)+1] colour per vertex, NULL = computed
  *   flags           VBD_MATERIAL_* | VBD_PRECISION_* | VBD_MODE_* | ...
- *   tpv             lanes per vertex (1,2,4,8,16,32), 0 = pick automatically
+ *   tpv             lanes per vertex (2, 4, 8, 16), 0 = pick automatically
  *   block_threads   threads per block, 0 = pick automatically
  *   device          CUDA device ordinal */
 int vbd_create(const double* rest_positions, int n_vertices, const int32_t* tets, int n_tets,
@@ -150,6 +155,11 @@ typedef struct vbd_info_t {
   int mode, tpv, block_threads, precision, material;
   long long n_slots, n_slot_records; /* incident (vertex, tet) pairs; padded records */
   long long device_bytes;
+  int n_unique_records; /* entries of the shared slot-record table */
+  int record_format;    /* bytes per slot: 8 (16-bit ids) or 16 (32-bit ids) */
+  int cluster;          /* block mode: thread blocks per cluster */
+  int n_blocks;         /* block mode: blocks of the current work map (> n_env: some
+                           environments are split over a cluster) */
 } vbd_info_t;
 int vbd_get_info(vbd_solver* s, vbd_info_t* info);
 

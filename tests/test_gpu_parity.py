@@ -127,6 +127,44 @@ def test_batched_uneven_envs_match_per_env_oracle():
     assert len(set(its.tolist())) >= 1
 
 
+@pytest.mark.parametrize("cluster", [2, 4, 8])
+def test_single_env_split_over_a_cluster(cluster):
+    """Block mode with the mesh replicated in every block of a cluster: each
+    block updates its share of a colour and broadcasts it through distributed
+    shared memory."""
+    s = scenes.cantilever(40)
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 30, mode="block", cluster=cluster)
+    inf = gpu.info()
+    assert inf["cluster"] == cluster and inf["n_blocks"] == cluster
+    assert worst < POS_TOL, worst
+    assert np.abs(ig - io).max() <= 2, (ig, io)
+
+
+def test_batched_heavy_environment_split():
+    """A large soft environment among small stiff ones: after the first step
+    the planner gives it a whole cluster; results match the oracle per
+    environment and the unsplit run."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = [scenes.mass_spring(15, 30, youngs=1e5, poisson=0.45)]
+    envs += [scenes.mass_spring(7, 5, youngs=1e6) for _ in range(7)]
+    split = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, cluster=4)
+    plain = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, cluster=1)
+    orcs = [oracle.OracleSolver(**e.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7,
+                                max_iter=1000, guarded=True) for e in envs]
+    for k in range(15):
+        its = split.step(1e-3)
+        its_plain = plain.step(1e-3)
+        x, xp = split.positions(), plain.positions()
+        for e, (env, o) in enumerate(zip(envs, orcs)):
+            xo = o.step(None, 1e-3)
+            sl = split.env_slice(e)
+            assert np.abs(x[sl] - xo).max() / _diag(env.vertices) < POS_TOL, (k, e)
+            assert abs(int(its[e]) - o.last_iterations) <= 2
+        assert np.abs(x - xp).max() < 1e-9
+        assert np.array_equal(its, its_plain)
+    assert split.info()["n_blocks"] > len(envs)   # the heavy environment was split
+
+
 def test_step_api_semantics():
     from warpvbd_b200 import VBDSolver
     s = scenes.cantilever(20)

@@ -39,6 +39,7 @@ MODE_GRAPH = 0x200
 MODE_HOSTLOOP = 0x300
 ORDER_INDEX = 0x1000
 STRICT_SPD = 0x2000
+CLUSTER_SHIFT = 16
 
 MODES = {"auto": MODE_AUTO, "block": MODE_BLOCK, "graph": MODE_GRAPH, "hostloop": MODE_HOSTLOOP}
 
@@ -54,7 +55,8 @@ class VBDInfo(ctypes.Structure):
         "n_vertices", "n_tets", "n_env", "n_colors", "max_valence", "mode", "tpv",
         "block_threads", "precision", "material")] + [
         ("n_slots", ctypes.c_longlong), ("n_slot_records", ctypes.c_longlong),
-        ("device_bytes", ctypes.c_longlong)]
+        ("device_bytes", ctypes.c_longlong), ("n_unique_records", ctypes.c_int),
+        ("record_format", ctypes.c_int), ("cluster", ctypes.c_int), ("n_blocks", ctypes.c_int)]
 
 
 # every entry point declared in include/vbd_b200.h: name -> (restype, argtypes)

@@ -23,7 +23,9 @@ class BatchedVBDSolver:
 
     def __init__(self, envs, damping_coefficient=0.0, gravity=(0.0, 0.0, -9.81), dx_tol=1e-7,
                  max_iter=1000, device="cuda", *, material="snh", precision="mixed",
-                 tpv=0, block_threads=0, order_index=False):
+                 tpv=0, block_threads=0, cluster=0, order_index=False):
+        """``cluster``: blocks per thread-block cluster (0 = automatic); an
+        environment much heavier than the others runs on a whole cluster."""
         Xs, Ts, rho, E, nu, act = [], [], [], [], [], []
         voff, toff = [0], [0]
         for env in envs:
@@ -50,6 +52,7 @@ class BatchedVBDSolver:
         flags = {"snh": _lib.MATERIAL_SNH, "stvk": _lib.MATERIAL_STVK}[material]
         flags |= _lib.PRECISIONS[precision]
         flags |= _lib.MODE_BLOCK
+        flags |= int(cluster) << _lib.CLUSTER_SHIFT
         if order_index:
             flags |= _lib.ORDER_INDEX
         L = _lib.load()

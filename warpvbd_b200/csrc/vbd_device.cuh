@@ -23,6 +23,12 @@ template <typename Real>
 using real4 = typename V4<Real>::type;
 
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
+__device__ __forceinline__ double4 ldcg4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldcg(q), b = __ldcg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
 __device__ __forceinline__ double4 ldg4(const double4* p) {
   const double2* q = reinterpret_cast<const double2*>(p);
   double2 a = __ldg(q), b = __ldg(q + 1);
@@ -197,13 +203,54 @@ __device__ __forceinline__ StepConst make_const(const StepParams& p) {
 }
 
 // ---------------------------------------------------------------------------
-// One warp processes one chunk (32/TPV vertices of one colour).  `ul` indexes
-// the environment's displacements by environment-local id (shared memory in
-// block mode, global memory in grid mode).
+// State accessors: environment-local vertex ids -> displacement.
+// SmemState: packed xyz (3 values per vertex) in shared memory (block mode).
+// GlobalState: Real4 per vertex in global memory (grid mode).
 // ---------------------------------------------------------------------------
-template <typename Real, typename SReal, int TPV, int MAT, bool SMEM>
+template <typename SReal>
+struct SmemState {
+  SReal* p;
+  __device__ __forceinline__ real4<SReal> load(int i) const {
+    real4<SReal> v;
+    v.x = p[3 * i];
+    v.y = p[3 * i + 1];
+    v.z = p[3 * i + 2];
+    v.w = SReal(0);
+    return v;
+  }
+  __device__ __forceinline__ void store(int i, const real4<SReal>& v) const {
+    p[3 * i] = v.x;
+    p[3 * i + 1] = v.y;
+    p[3 * i + 2] = v.z;
+  }
+};
+
+template <typename SReal>
+struct GlobalState {
+  real4<SReal>* p;
+  // neighbours of other colours are not written during a colour's kernel, and
+  // the vertex's own value was written by an earlier kernel: the read-only
+  // path is safe
+  __device__ __forceinline__ real4<SReal> load(int i) const { return ldg4(p + i); }
+  __device__ __forceinline__ void store(int i, const real4<SReal>& v) const { p[i] = v; }
+};
+
+template <int FMT>
+__device__ __forceinline__ int4 load_slot(const DevMesh& m, size_t i) {
+  if (FMT == kFmtIdx16) {
+    const ushort4 s = __ldg(m.rec_idx16 + i);
+    return make_int4(s.x, s.y, s.z, s.w);
+  }
+  return __ldg(m.rec_idx + i);
+}
+
+// ---------------------------------------------------------------------------
+// One warp processes one chunk (32/TPV vertices of one colour).  `st` reads
+// and writes the environment's displacements by environment-local id.
+// ---------------------------------------------------------------------------
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
 __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const ColorInfo& ci,
-                                              int q, int lane, real4<SReal>* ul,
+                                              int q, int lane, const State& st,
                                               const StepConst& sc, unsigned long long& cmax,
                                               unsigned& stat) {
   using R4 = real4<Real>;
@@ -219,29 +266,23 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
   uo.x = uo.y = uo.z = uo.w = SReal(0);
   if (valid) {
     k = __ldg(m.valence + gv);
-    uo = SMEM ? ul[lv] : ldg4(ul + lv);
+    uo = st.load(lv);
   }
   Real g[3] = {Real(0), Real(0), Real(0)};
   Real h[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
-  const int4* ridx = m.rec_idx + (size_t)ch.block * 32 + lane;
-  const R4* rval = reinterpret_cast<const R4*>(m.rec_val) + (size_t)ch.block * 96 + lane;
+  const R4* tab = reinterpret_cast<const R4*>(m.rec_tab);
+  const size_t base = (size_t)ch.block * 32 + lane;
 #pragma unroll 2
   for (int s = 0; s < ch.steps; ++s) {
     if (s * TPV + sub < k) {
-      const int4 id = __ldg(ridx + (size_t)s * 32);
-      const R4 q0 = ldg4(rval + (size_t)s * 96);
-      const R4 q1 = ldg4(rval + (size_t)s * 96 + 32);
-      const R4 q2 = ldg4(rval + (size_t)s * 96 + 64);
-      S4 a, b, c;
-      if (SMEM) {
-        a = ul[id.x];
-        b = ul[id.y];
-        c = ul[id.z];
-      } else {
-        a = ldg4(ul + id.x);
-        b = ldg4(ul + id.y);
-        c = ldg4(ul + id.z);
-      }
+      const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
+      const R4* t = tab + 3 * (size_t)id.w;
+      const R4 q0 = ldg4(t);
+      const R4 q1 = ldg4(t + 1);
+      const R4 q2 = ldg4(t + 2);
+      const S4 a = st.load(id.x);
+      const S4 b = st.load(id.y);
+      const S4 c = st.load(id.z);
       // neighbour offsets formed in the state precision, then rounded
       slot_accumulate<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
                                  Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
@@ -257,7 +298,9 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
     for (int i = 0; i < 6; ++i) h[i] += __shfl_xor_sync(0xffffffffu, h[i], off);
   }
   if (valid && sub == 0) {
-    const S4 tt = ldg4(reinterpret_cast<const S4*>(m.ut) + gv);
+    // ut / up are written in this launch by another block of a group: read
+    // them through L2, past a possibly stale L1 line
+    const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
     const Real mdt2 = Real(tt.w * SReal(sc.inv_dt2));
     Real G[3], H[6];
     G[0] = g[0] + mdt2 * Real(uo.x - tt.x);
@@ -265,7 +308,7 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
     G[2] = g[2] + mdt2 * Real(uo.z - tt.z);
     if (sc.damp) {
       // Rayleigh-like damping kd * H_el (x - x_prev) / dt (vbd_solver.py:222-223)
-      const S4 u0 = ldg4(reinterpret_cast<const S4*>(m.up) + gv);
+      const S4 u0 = ldcg4(reinterpret_cast<const S4*>(m.up) + gv);
       const Real kd = Real(sc.kd_dt);
       const Real ex = Real(uo.x - u0.x), ey = Real(uo.y - u0.y), ez = Real(uo.z - u0.z);
       G[0] += kd * (h[0] * ex + h[1] * ey + h[2] * ez);
@@ -295,7 +338,7 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
     un.x += SReal(dx[0]);
     un.y += SReal(dx[1]);
     un.z += SReal(dx[2]);
-    ul[lv] = un;
+    st.store(lv, un);
     const double c = fabs(double(dx[0] + dx[1] + dx[2]));
     if (!isfinite(c)) stat |= kStatNonFinite;
     const unsigned long long cb = conv_bits(c);
@@ -305,10 +348,10 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
 
 // Inertia target and initial guess (position_initialization,
 // vbd_solver.py:277-292): ut = u + dt v + dt^2 g (w keeps the lumped mass),
-// up = u, and active vertices start from ut.
+// up = u (written when write_back), and active vertices start from ut.
 template <typename Real>
 __device__ __forceinline__ real4<Real> begin_vertex(const DevMesh& m, int gv, bool active,
-                                                    const StepConst& sc) {
+                                                    const StepConst& sc, bool write_back) {
   using R4 = real4<Real>;
   R4* U = reinterpret_cast<R4*>(m.u);
   R4* UT = reinterpret_cast<R4*>(m.ut);
@@ -321,8 +364,10 @@ __device__ __forceinline__ real4<Real> begin_vertex(const DevMesh& m, int gv, bo
   tt.x = u0.x + v0.x * dt + Real(sc.g[0]) * dt2;
   tt.y = u0.y + v0.y * dt + Real(sc.g[1]) * dt2;
   tt.z = u0.z + v0.z * dt + Real(sc.g[2]) * dt2;
-  UT[gv] = tt;
-  UP[gv] = u0;
+  if (write_back) {
+    UT[gv] = tt;
+    UP[gv] = u0;
+  }
   R4 un = u0;
   if (active) {
     un.x = tt.x;
@@ -345,6 +390,43 @@ __device__ __forceinline__ void end_vertex(const DevMesh& m, int gv, const real4
   v.z = (un.z - u0.z) * idt;
   v.w = Real(0);
   reinterpret_cast<R4*>(m.vel)[gv] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Runtime (precision, material, record format, lanes per vertex) -> template
+// instantiation: calls f.template run<Real, SReal, TPV, MAT, FMT>().
+template <typename Real, typename SReal, int MAT, int FMT, class F>
+cudaError_t dispatch_tpv(int tpv, F& f) {
+  switch (tpv) {
+    case 2: return f.template run<Real, SReal, 2, MAT, FMT>();
+    case 4: return f.template run<Real, SReal, 4, MAT, FMT>();
+    case 8: return f.template run<Real, SReal, 8, MAT, FMT>();
+    case 16: return f.template run<Real, SReal, 16, MAT, FMT>();
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename Real, typename SReal, int MAT, class F>
+cudaError_t dispatch_fmt(int fmt, int tpv, F& f) {
+  if (fmt == kFmtIdx16) return dispatch_tpv<Real, SReal, MAT, kFmtIdx16>(tpv, f);
+  if (fmt == kFmtIdx32) return dispatch_tpv<Real, SReal, MAT, kFmtIdx32>(tpv, f);
+  return cudaErrorInvalidValue;
+}
+
+template <typename Real, typename SReal, class F>
+cudaError_t dispatch_mat(int material, int fmt, int tpv, F& f) {
+  return material == kSNH ? dispatch_fmt<Real, SReal, kSNH>(fmt, tpv, f)
+                          : dispatch_fmt<Real, SReal, kStVK>(fmt, tpv, f);
+}
+
+template <class F>
+cudaError_t dispatch(int prec, int material, int fmt, int tpv, F& f) {
+  switch (prec) {
+    case 0: return dispatch_mat<float, float>(material, fmt, tpv, f);
+    case 1: return dispatch_mat<float, double>(material, fmt, tpv, f);
+    case 2: return dispatch_mat<double, double>(material, fmt, tpv, f);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace vbd

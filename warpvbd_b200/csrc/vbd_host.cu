@@ -16,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/vbd_b200.h"
@@ -148,12 +149,54 @@ int build_tet_data(const double* X, const int32_t* tets, int T, const double* rh
   return VBD_OK;
 }
 
+// Unique slot-record values (b_n0, p0, b_n1, p1, b_n2, p2).  Two slots share an
+// entry when their values are bitwise equal after conversion to the solver's
+// arithmetic precision, so sharing never changes a result.  Voxel meshes have
+// a handful of tet shapes, so thousands of slots map to one entry.
+struct RecordTable {
+  bool fp64 = false;
+  std::vector<double> vals;  // 12 per entry
+  struct Key {
+    uint64_t w[12];
+    bool operator==(const Key& o) const { return std::memcmp(w, o.w, sizeof w) == 0; }
+  };
+  struct KeyHash {
+    size_t operator()(const Key& k) const {
+      uint64_t h = 1469598103934665603ull;
+      for (uint64_t x : k.w) h = (h ^ x) * 1099511628211ull;
+      return (size_t)(h ^ (h >> 29));
+    }
+  };
+  std::unordered_map<Key, int, KeyHash> index;
+
+  int insert(const double* v) {
+    Key k;
+    for (int i = 0; i < 12; ++i) {
+      if (fp64) {
+        std::memcpy(&k.w[i], &v[i], 8);
+      } else {
+        const float f = (float)v[i];
+        uint32_t b;
+        std::memcpy(&b, &f, 4);
+        k.w[i] = b;
+      }
+    }
+    auto it = index.find(k);
+    if (it != index.end()) return it->second;
+    const int id = (int)(vals.size() / 12);
+    vals.insert(vals.end(), v, v + 12);
+    index.emplace(k, id);
+    return id;
+  }
+  int size() const { return (int)(vals.size() / 12); }
+};
+
 struct Layout {
   std::vector<EnvInfo> env;
   std::vector<ColorInfo> color;
   std::vector<ChunkInfo> chunk;
-  std::vector<int4> rec_idx;
-  std::vector<double> rec_val;  // [block][plane][lane][4]
+  std::vector<int4> rec_idx;  // (n0, n1, n2, record id)
+  RecordTable table;
   std::vector<int> valence;     // new id
   std::vector<double> mass;     // new id
   std::vector<int> new_of_old;
@@ -297,10 +340,9 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
       for (int s = off[v]; s < off[v + 1]; ++s) m += td.mass[to + inc[s]] / 4.0;
       L.mass[gnew] = m;
     }
-    // slot records
+    // slot records: (n0, n1, n2, record id) per slot, the record values in a
+    // table shared by every slot with the same values in the solver precision
     L.rec_idx.resize((size_t)block_count * 32, make_int4(0, 0, 0, 0));
-    L.rec_val.resize((size_t)block_count * 32 * 12, 0.0);
-    // fill records by walking solved vertices in new order
     std::vector<int> old_of_new_local(vn);
     for (int v = 0; v < vn; ++v) old_of_new_local[new_local[v]] = v;
     for (int ci_i = ei.cbase; ci_i < ei.cbase + ei.ncolors; ++ci_i) {
@@ -320,22 +362,21 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
             const int a = loc[off[ov] + j];
             const size_t blk = (size_t)ch.block + s;
             int ids[3];
+            double val[12];
             const double* bt = &td.b[(size_t)t * 12];
             const double* pt = &td.p[(size_t)t * 3];
-            double* val = &L.rec_val[(blk * 3 * 32) * 4];
             int n = 0;
             for (int qq = 0; qq < 4; ++qq) {
               if (qq == a) continue;
-              const int other_old = tets[4 * (size_t)t + qq] - vo;
-              ids[n] = new_local[other_old];
-              double* pv = val + ((size_t)n * 32 + lane) * 4;
-              pv[0] = bt[qq * 3 + 0];
-              pv[1] = bt[qq * 3 + 1];
-              pv[2] = bt[qq * 3 + 2];
-              pv[3] = pt[n];
+              ids[n] = new_local[tets[4 * (size_t)t + qq] - vo];
+              val[4 * n + 0] = bt[qq * 3 + 0];
+              val[4 * n + 1] = bt[qq * 3 + 1];
+              val[4 * n + 2] = bt[qq * 3 + 2];
+              val[4 * n + 3] = pt[n];
               ++n;
             }
-            L.rec_idx[blk * 32 + lane] = make_int4(ids[0], ids[1], ids[2], 0);
+            const int rid = L.table.insert(val);
+            L.rec_idx[blk * 32 + lane] = make_int4(ids[0], ids[1], ids[2], rid);
             L.n_slots++;
           }
         }
@@ -366,13 +407,22 @@ struct vbd_solver {
   DevBuf<ColorInfo> d_color;
   DevBuf<ChunkInfo> d_chunk;
   DevBuf<int4> d_rec_idx;
-  DevBuf<unsigned char> d_rec_val;
+  DevBuf<ushort4> d_rec_idx16;
+  DevBuf<unsigned char> d_rec_tab;
+  int fmt = kFmtIdx32;
   DevBuf<int> d_valence, d_map, d_iters;
   DevBuf<unsigned> d_status;
   DevBuf<unsigned char> d_u, d_ut, d_up, d_vel;
   DevBuf<double> d_X, d_io, d_tol;
   DevBuf<StepParams> d_params;
   DevBuf<LoopControl> d_ctl;
+  // block-mode work map: (environment, rank, group size) per thread block
+  int cluster = 1;           // blocks per cluster = group size of a split environment
+  bool replan = false;       // re-plan from the measured sweep counts after each step
+  int capacity_blocks = 0;   // resident blocks on the device for this launch shape
+  std::vector<double> env_work;  // incident slots per environment
+  std::vector<int4> work;
+  DevBuf<int4> d_work;
   // pinned host
   int* h_iters = nullptr;
   unsigned* h_status = nullptr;
@@ -392,7 +442,9 @@ struct vbd_solver {
     m.color = d_color.p;
     m.chunk = d_chunk.p;
     m.rec_idx = d_rec_idx.p;
-    m.rec_val = d_rec_val.p;
+    m.rec_idx16 = d_rec_idx16.p;
+    m.rec_tab = d_rec_tab.p;
+    m.fmt = fmt;
     m.valence = d_valence.p;
     m.u = d_u.p;
     m.ut = d_ut.p;
@@ -420,7 +472,8 @@ void free_solver(vbd_solver* s) {
   s->d_color.release();
   s->d_chunk.release();
   s->d_rec_idx.release();
-  s->d_rec_val.release();
+  s->d_rec_idx16.release();
+  s->d_rec_tab.release();
   s->d_valence.release();
   s->d_map.release();
   s->d_iters.release();
@@ -432,6 +485,7 @@ void free_solver(vbd_solver* s) {
   s->d_X.release();
   s->d_io.release();
   s->d_tol.release();
+  s->d_work.release();
   s->d_params.release();
   s->d_ctl.release();
   if (s->h_iters) cudaFreeHost(s->h_iters);
@@ -456,6 +510,77 @@ struct DeviceGuard {
   }
 };
 
+// Block-mode work map.  Each environment's work estimate is its slot count
+// times its last sweep count (1 before the first step).  With cluster > 1 the
+// heaviest environments may each take a whole cluster (group = cluster); the
+// others take one block each, packed `cluster` to a cluster, heaviest first.
+// The split set is the one with the smallest predicted step time: the
+// largest of (heaviest single-block environment, heaviest split environment
+// / (cluster * efficiency), total work / resident blocks).
+void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work) {
+  const int n = s->n_env, C = s->cluster;
+  std::vector<double> w(n);
+  for (int e = 0; e < n; ++e) w[e] = s->env_work[e] * std::max(1, iters ? iters[e] : 1);
+  std::vector<int> order(n);
+  for (int e = 0; e < n; ++e) order[e] = e;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
+  work.clear();
+  if (C <= 1) {
+    for (int e : order) work.push_back(make_int4(e, 0, 1, 0));
+    return;
+  }
+  if (n == 1) {
+    for (int r = 0; r < C; ++r) work.push_back(make_int4(0, r, C, 0));
+    return;
+  }
+  // parallel efficiency of a split environment (cluster barriers and the
+  // replica broadcasts cost a share of the gain)
+  const double eff = C == 2 ? 0.85 : (C == 4 ? 0.75 : (C == 8 ? 0.6 : 0.45));
+  const double cap = std::max(1, s->capacity_blocks);
+  double total = 0.0;
+  for (double x : w) total += x;
+  int best_h = 0;
+  double best_t = 1e300, extra = 0.0;
+  for (int h = 0; h <= n; ++h) {
+    // the h heaviest environments are split
+    if (h > 0) extra += w[order[h - 1]] * (1.0 / eff - 1.0);
+    const double blocks = (double)(n - h) + (double)h * C;
+    const double t_split = h > 0 ? w[order[0]] / (C * eff) : 0.0;
+    const double t_single = h < n ? w[order[h]] : 0.0;
+    const double t_fill = (total + extra) / std::min(cap, blocks);
+    const double t = std::max(std::max(t_split, t_single), t_fill);
+    if (t < best_t * 0.999) {
+      best_t = t;
+      best_h = h;
+    }
+    if (t_single <= t_split) break;  // splitting more cannot help
+  }
+  for (int i = 0; i < best_h; ++i)
+    for (int r = 0; r < C; ++r) work.push_back(make_int4(order[i], r, C, 0));
+  int in_cluster = 0;
+  for (int i = best_h; i < n; ++i) {
+    work.push_back(make_int4(order[i], 0, 1, 0));
+    in_cluster = (in_cluster + 1) % C;
+  }
+  while (in_cluster != 0) {
+    work.push_back(make_int4(-1, 0, 0, 0));
+    in_cluster = (in_cluster + 1) % C;
+  }
+}
+
+int upload_plan(vbd_solver* s, const int* iters) {
+  std::vector<int4> w;
+  make_plan(s, iters, w);
+  if (w.size() == s->work.size() &&
+      std::memcmp(w.data(), s->work.data(), w.size() * sizeof(int4)) == 0)
+    return VBD_OK;
+  if (w.size() > s->d_work.n) return fail(VBD_ERR_CUDA, "work map larger than its buffer");
+  // the stream is idle here (create, or after a synchronising step)
+  CUDA_TRY(cudaMemcpy(s->d_work.p, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  s->work.swap(w);
+  return VBD_OK;
+}
+
 int create_impl(const double* X, int V, const int32_t* tets, int T, const double* rho,
                 const double* E, const double* nu, const uint8_t* active, double kd,
                 const double* gravity, const int32_t* coloring, const std::vector<int>& voff,
@@ -468,8 +593,8 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   for (size_t i = 0; i < 4 * (size_t)T; ++i)
     if (tets[i] < 0 || tets[i] >= V)
       return fail(VBD_ERR_INVALID_ARG, "tet vertex id out of range");
-  if (tpv != 0 && tpv != 1 && tpv != 2 && tpv != 4 && tpv != 8 && tpv != 16 && tpv != 32)
-    return fail(VBD_ERR_INVALID_ARG, "tpv must be 1, 2, 4, 8, 16 or 32");
+  if (tpv != 0 && tpv != 2 && tpv != 4 && tpv != 8 && tpv != 16)
+    return fail(VBD_ERR_INVALID_ARG, "tpv must be 2, 4, 8 or 16");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(VBD_ERR_NO_DEVICE, "no CUDA device");
@@ -501,7 +626,9 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   // provisional environment size bound for the shared-memory check
   int max_env_v = 0;
   for (int e = 0; e < s->n_env; ++e) max_env_v = std::max(max_env_v, voff[e + 1] - voff[e]);
-  const size_t smem_need = (size_t)max_env_v * s->real4_bytes;
+  // block mode keeps x, y, z of every vertex of the environment in shared memory
+  const size_t smem_per_vertex = s->state64 ? 24 : 12;
+  const size_t smem_need = (size_t)max_env_v * smem_per_vertex;
   const bool fits = smem_need <= (size_t)env_kernel_max_smem();
   if (mode == VBD_MODE_AUTO) {
     if (s->n_env > 1)
@@ -519,6 +646,13 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   }
   s->mode = mode;
   const bool block_mode = mode == VBD_MODE_BLOCK;
+  const int cl = (flags >> VBD_CLUSTER_SHIFT) & 0x1F;
+  if (cl != 0 && cl != 1 && cl != 2 && cl != 4 && cl != 8 && cl != 16) {
+    delete s;
+    return fail(VBD_ERR_INVALID_ARG, "cluster size must be 1, 2, 4, 8 or 16");
+  }
+  s->cluster = !block_mode ? 1 : (cl ? cl : (s->n_env > 1 ? 4 : 1));
+  s->replan = block_mode && s->n_env > 1 && s->cluster > 1;
   if (threads == 0) threads = block_mode ? (s->n_env > 1 ? 256 : 512) : 256;
   if (!block_mode) threads = 256;
   if (threads % 32 || threads < 32 || threads > 512) {
@@ -541,22 +675,25 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
       for (int v = 0; v < nvc; ++v)
         if (col[v] >= 0) cnt[col[v]]++;
       const int mg = std::max(1, *std::max_element(cnt.begin(), cnt.end()));
-      tpv = 1;
-      while (tpv < 32 && mg * tpv * 2 <= threads) tpv *= 2;
-      if (tpv < 2) tpv = 2;
+      tpv = 2;
+      while (tpv < 16 && mg * tpv * 2 <= threads) tpv *= 2;
     } else {
       tpv = 4;  // batched environments and the grid-mode colour kernels
     }
   }
   s->tpv = tpv;
+  s->L.table.fp64 = s->fp64;
   rc = build_layout(X, V, tets, T, active, voff, toff, coloring, td, tpv,
                     (flags & VBD_ORDER_INDEX) != 0, s->L);
   if (rc != VBD_OK) {
     delete s;
     return rc;
   }
-  s->smem_bytes = (size_t)s->L.max_env_vertices * s->real4_bytes;
+  s->smem_bytes = (size_t)s->L.max_env_vertices * smem_per_vertex;
   s->n_records = (long long)s->L.rec_idx.size();
+  // 16-bit slots when every environment-local id and record id fits
+  s->fmt = (s->L.max_env_vertices <= 65536 && s->L.table.size() <= 65536) ? kFmtIdx16
+                                                                            : kFmtIdx32;
 
   // ---- device upload --------------------------------------------------------
   auto bad = [&](cudaError_t e, const char* what) {
@@ -571,27 +708,40 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   if (!err && bad(s->d_env.upload(L.env, st), "env")) err = 1;
   if (!err && bad(s->d_color.upload(L.color, st), "color")) err = 1;
   if (!err && bad(s->d_chunk.upload(L.chunk, st), "chunk")) err = 1;
-  if (!err && bad(s->d_rec_idx.upload(L.rec_idx, st), "rec_idx")) err = 1;
   if (!err) {
-    // record values in the solver precision
-    const size_t nval = L.rec_val.size();
+    if (s->fmt == kFmtIdx16) {
+      std::vector<ushort4> r16(L.rec_idx.size());
+      for (size_t i = 0; i < r16.size(); ++i) {
+        const int4 r = L.rec_idx[i];
+        r16[i] = make_ushort4((unsigned short)r.x, (unsigned short)r.y, (unsigned short)r.z,
+                              (unsigned short)r.w);
+      }
+      if (bad(s->d_rec_idx16.upload(r16, st), "rec_idx16")) err = 1;
+      if (!err) cudaStreamSynchronize(st);  // r16 goes out of scope
+    } else if (bad(s->d_rec_idx.upload(L.rec_idx, st), "rec_idx")) {
+      err = 1;
+    }
+  }
+  if (!err) {
+    // record table in the solver precision: 3 Real4 per entry
+    const size_t nval = L.table.vals.size();
     if (s->fp64) {
-      if (bad(s->d_rec_val.alloc(nval * 8), "rec_val")) err = 1;
+      if (bad(s->d_rec_tab.alloc(nval * 8), "rec_tab")) err = 1;
       if (!err && nval &&
-          bad(cudaMemcpyAsync(s->d_rec_val.p, L.rec_val.data(), nval * 8, cudaMemcpyHostToDevice,
-                              st),
-              "rec_val copy"))
+          bad(cudaMemcpyAsync(s->d_rec_tab.p, L.table.vals.data(), nval * 8,
+                              cudaMemcpyHostToDevice, st),
+              "rec_tab copy"))
         err = 1;
     } else {
       std::vector<float> f(nval);
-      for (size_t i = 0; i < nval; ++i) f[i] = (float)L.rec_val[i];
-      if (bad(s->d_rec_val.alloc(nval * 4), "rec_val")) err = 1;
+      for (size_t i = 0; i < nval; ++i) f[i] = (float)L.table.vals[i];
+      if (bad(s->d_rec_tab.alloc(nval * 4), "rec_tab")) err = 1;
       if (!err && nval &&
-          bad(cudaMemcpyAsync(s->d_rec_val.p, f.data(), nval * 4, cudaMemcpyHostToDevice, st),
-              "rec_val copy"))
+          bad(cudaMemcpyAsync(s->d_rec_tab.p, f.data(), nval * 4, cudaMemcpyHostToDevice, st),
+              "rec_tab copy"))
         err = 1;
-      if (!err) cudaStreamSynchronize(st);  // f goes out of scope
     }
+    if (!err) cudaStreamSynchronize(st);  // staging vectors go out of scope
   }
   if (!err && bad(s->d_valence.upload(L.valence, st), "valence")) err = 1;
   if (!err && bad(s->d_map.upload(L.new_of_old, st), "map")) err = 1;
@@ -641,12 +791,33 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
                   "pinned"))
     err = 1;
   if (!err && bad(cudaStreamSynchronize(st), "setup sync")) err = 1;
+  if (!err && block_mode) {
+    // work estimate per environment: its incident (vertex, tet) slots
+    s->env_work.assign(s->n_env, 0.0);
+    for (int e = 0; e < s->n_env; ++e) s->env_work[e] = 4.0 * (toff[e + 1] - toff[e]) + 1.0;
+    int occ = 0;
+    if (bad(env_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads, s->smem_bytes,
+                          s->cluster, &occ),
+            "occupancy"))
+      err = 1;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    s->capacity_blocks = s->cluster > 1 ? occ * s->cluster : occ * sms;
+    if (!err && s->capacity_blocks < 1) {
+      g_last_error = "block mode: this launch shape does not fit on the device";
+      err = 1;
+    }
+    if (!err && bad(s->d_work.alloc((size_t)s->n_env * s->cluster + s->cluster), "work"))
+      err = 1;
+    if (!err && upload_plan(s, nullptr) != VBD_OK) err = 1;
+  }
   if (err) {
     free_solver(s);
     return VBD_ERR_CUDA;
   }
   s->device_bytes = 0;
-  s->device_bytes += (long long)(s->d_rec_idx.n * sizeof(int4) + s->d_rec_val.n);
+  s->device_bytes += (long long)(s->d_rec_idx.n * sizeof(int4) +
+                                 s->d_rec_idx16.n * sizeof(ushort4) + s->d_rec_tab.n);
   s->device_bytes += (long long)(4 * sb + s->d_X.n * 8 + s->d_io.n * 8);
   s->device_bytes += (long long)(s->d_valence.n * 4 + s->d_map.n * 4);
   *out = s;
@@ -753,7 +924,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
       dtol = s->d_tol.p;
     }
     CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
-                             s->n_env, s->smem_bytes, st));
+                             s->d_work.p, (int)s->work.size(), s->cluster, s->smem_bytes, st));
   } else if (s->mode == VBD_MODE_GRAPH) {
     rc = build_graph(s);
     if (rc != VBD_OK) return rc;
@@ -790,6 +961,11 @@ int finish(vbd_solver* s, int* iters_out) {
   s->pending = false;
   if (iters_out) std::memcpy(iters_out, s->h_iters, sizeof(int) * s->n_env);
   s->last_status = status_from_bits(s, s->h_status);
+  if (s->replan) {
+    // re-balance the next step from this step's sweep counts (stream is idle)
+    const int rc = upload_plan(s, s->h_iters);
+    if (rc != VBD_OK) return rc;
+  }
   return s->last_status;
 }
 
@@ -978,6 +1154,10 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
   info->n_slots = s->L.n_slots;
   info->n_slot_records = s->n_records;
   info->device_bytes = s->device_bytes;
+  info->n_unique_records = s->L.table.size();
+  info->record_format = s->fmt == kFmtIdx16 ? 8 : 16;
+  info->cluster = s->cluster;
+  info->n_blocks = (int)s->work.size();
   return VBD_OK;
 }
 

@@ -72,12 +72,20 @@ struct LoopControl {
   unsigned status;
 };
 
+// Slot record formats (both index a table of unique (b_n0, b_n1, b_n2, p)
+// records, 3 Real4 each, so slots that share a tet shape and material share
+// one table entry):
+//   kFmtIdx32  int4    (n0, n1, n2, record id)                     16 B/slot
+//   kFmtIdx16  ushort4 (n0, n1, n2, record id), all values < 65536  8 B/slot
+enum RecordFormat : int { kFmtIdx32 = 1, kFmtIdx16 = 2 };
+
 struct DevMesh {
   const EnvInfo* env;
   const ColorInfo* color;
   const ChunkInfo* chunk;
-  const int4* rec_idx;
-  const void* rec_val;  // Real4
+  const int4* rec_idx;       // kFmtIdx32 slots
+  const ushort4* rec_idx16;  // kFmtIdx16 slots
+  const void* rec_tab;       // Real4 [n_unique][3]
   const int* valence;   // per global vertex
   void* u;              // Real4
   void* ut;
@@ -87,6 +95,7 @@ struct DevMesh {
   unsigned* status;     // per env
   int n_env;
   int n_vertices;
+  int fmt;  // RecordFormat
 };
 
 }  // namespace vbd

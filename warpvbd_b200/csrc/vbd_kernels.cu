@@ -22,6 +22,7 @@
 // using lambda'(alpha-1) = 3/4 mu', cof(F) = (1+tr G) I - G^T + cof(G) and
 // J-1 = tr G + (tr(G)^2 - tr(G^2))/2 + det G.  StVK (vbd_solver.py:127-144)
 // uses E = (G + G^T + G^T G)/2 in the same way.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -32,67 +33,166 @@
 namespace vbd {
 
 // ---------------------------------------------------------------------------
-// Block mode: blockIdx.x = environment.  The environment's displacements live
-// in shared memory for the whole step; colours are separated by
-// __syncthreads(); the convergence test is a block reduction.
+// Block mode.  Work item work[blockIdx.x] = (environment, rank, group size):
+// an environment runs on one thread block, or -- when it is much heavier
+// than the others -- on all `group` blocks of one thread-block cluster.  Every
+// block of a group holds a replica of the environment's positions (x, y, z)
+// in shared memory for the whole step, updates its share of every colour
+// (chunks rank, rank + group, ...) and writes each update into every replica
+// through distributed shared memory.  Colours are separated by
+// __syncthreads() (one block) or the cluster barrier (a group); the
+// convergence test is a block reduction followed, in a group, by an exchange
+// of the block maxima.  No block waits on a flag.
 // ---------------------------------------------------------------------------
-template <typename Real, typename SReal, int TPV, int MAT>
-__global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
-                                                        const double* __restrict__ tol_env) {
-  using S4 = real4<SReal>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S4* su = reinterpret_cast<S4*>(smem_raw);
-  __shared__ unsigned long long s_red[32];
-  __shared__ int s_done;
-  __shared__ unsigned s_stat;
-  const int env = blockIdx.x;
-  const EnvInfo e = m.env[env];
-  const StepConst sc = make_const(p);
-  const double tol = tol_env ? tol_env[env] : p.tol;
-  if (threadIdx.x == 0) s_stat = 0u;
-  for (int i = threadIdx.x; i < e.nv; i += blockDim.x)
-    su[i] = begin_vertex<SReal>(m, e.vbase + i, i < e.nact, sc);
-  __syncthreads();
+namespace cg = cooperative_groups;
+
+constexpr int kMaxGroup = 16;
+
+// Replicated environment state: loads from the block's own replica, stores
+// into every replica of the group (remote replicas through distributed shared
+// memory; map_shared_rank is one address-mapping instruction).
+template <typename SReal>
+struct GroupSmemState {
+  SReal* local;
+  int g, rank;
+  __device__ __forceinline__ real4<SReal> load(int i) const {
+    real4<SReal> v;
+    v.x = local[3 * i];
+    v.y = local[3 * i + 1];
+    v.z = local[3 * i + 2];
+    v.w = SReal(0);
+    return v;
+  }
+  __device__ __forceinline__ void store(int i, const real4<SReal>& v) const {
+    SReal* p = local + 3 * i;
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+    cg::cluster_group cl = cg::this_cluster();
+    for (int r = 0; r < g; ++r) {
+      if (r == rank) continue;
+      SReal* d = cl.map_shared_rank(p, r);
+      d[0] = v.x;
+      d[1] = v.y;
+      d[2] = v.z;
+    }
+  }
+};
+
+template <bool GROUP>
+__device__ __forceinline__ void group_sync(int g) {
+  if (GROUP && g > 1)
+    cg::this_cluster().sync();
+  else
+    __syncthreads();
+}
+
+// Sweeps of one environment until its convergence test passes or max_iter;
+// returns the number of sweeps.
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP, class State>
+__device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, const State& su,
+                                          int rank, int g, const StepConst& sc, int max_iter,
+                                          double tol, unsigned& stat, bool& converged,
+                                          unsigned long long* s_red,
+                                          unsigned long long (*s_conv)[kMaxGroup],
+                                          int* s_done) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  unsigned stat = 0u;
   int it = 0;
-  bool converged = false;
   for (;;) {
     unsigned long long cmax = 0ull;
     for (int c = 0; c < e.ncolors; ++c) {
       const ColorInfo ci = m.color[e.cbase + c];
-      for (int q = ci.chunk_begin + warp; q < ci.chunk_end; q += nwarps)
-        process_chunk<Real, SReal, TPV, MAT, true>(m, e.vbase, ci, q, lane, su, sc, cmax, stat);
-      __syncthreads();
+      for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
+        process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, su, sc, cmax, stat);
+      group_sync<GROUP>(g);
     }
     ++it;
     cmax = warp_max_u64(cmax);
     if (lane == 0) s_red[warp] = cmax;
     __syncthreads();
+    unsigned long long v = 0ull;
     if (warp == 0) {
-      unsigned long long v = lane < nwarps ? s_red[lane] : 0ull;
+      v = lane < nwarps ? s_red[lane] : 0ull;
       v = warp_max_u64(v);
-      if (lane == 0) {
-        const bool nan = v > 0x7ff0000000000000ull;
-        const bool conv = !nan && (__longlong_as_double((long long)v) < tol);
-        s_done = (conv ? 1 : 0) | ((nan || conv || it >= p.max_iter) ? 2 : 0);
+    }
+    if (GROUP && g > 1) {
+      // exchange the block maxima (double-buffered by sweep parity)
+      cg::cluster_group cl = cg::this_cluster();
+      if (threadIdx.x == 0)
+        for (int r = 0; r < g; ++r) *cl.map_shared_rank(&s_conv[it & 1][rank], r) = v;
+      cl.sync();
+      if (threadIdx.x == 0) {
+        v = 0ull;
+        for (int r = 0; r < g; ++r) v = s_conv[it & 1][r] > v ? s_conv[it & 1][r] : v;
       }
     }
+    if (threadIdx.x == 0) {
+      const bool nan = v > 0x7ff0000000000000ull;
+      const bool conv = !nan && (__longlong_as_double((long long)v) < tol);
+      *s_done = (conv ? 1 : 0) | ((nan || conv || it >= max_iter) ? 2 : 0);
+    }
     __syncthreads();
-    const int d = s_done;
+    const int d = *s_done;
     if (d & 2) {
       converged = d & 1;
-      break;
+      return it;
     }
   }
-  for (int i = threadIdx.x; i < e.nv; i += blockDim.x) {
-    const S4 un = su[i];
+}
+
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
+__global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
+                                                        const double* __restrict__ tol_env,
+                                                        const int4* __restrict__ work) {
+  using S4 = real4<SReal>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SReal* sp = reinterpret_cast<SReal*>(smem_raw);
+  __shared__ unsigned long long s_red[32];
+  __shared__ unsigned long long s_conv[2][kMaxGroup];
+  __shared__ int s_done;
+  __shared__ unsigned s_stat;
+  const int4 w = work[blockIdx.x];
+  const int env = w.x, rank = w.y, g = w.z;
+  if (env < 0) return;  // padding block of a cluster of single-block environments
+  const EnvInfo e = m.env[env];
+  const StepConst sc = make_const(p);
+  const double tol = tol_env ? tol_env[env] : p.tol;
+  if (threadIdx.x == 0) s_stat = 0u;
+  // every replica computes the inertia guess of every vertex; rank 0 writes
+  // the step-start state back
+  const SmemState<SReal> local{sp};
+  for (int i = threadIdx.x; i < e.nv; i += blockDim.x)
+    local.store(i, begin_vertex<SReal>(m, e.vbase + i, i < e.nact, sc, rank == 0));
+  unsigned stat = 0u;
+  bool converged = false;
+  int it;
+  if (GROUP && g > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    const GroupSmemState<SReal> su{sp, g, rank};
+    cl.sync();  // every block of the group has started and filled its replica
+    it = env_sweeps<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, su, rank, g, sc, p.max_iter, tol,
+                                                        stat, converged, s_red, s_conv, &s_done);
+  } else {
+    __syncthreads();
+    it = env_sweeps<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, p.max_iter, tol,
+                                                        stat, converged, s_red, s_conv, &s_done);
+  }
+  // velocity update and write-back, vertices split over the group
+  for (int i = rank + g * threadIdx.x; i < e.nv; i += g * blockDim.x) {
+    S4 un = local.load(i);
+    un.w = reinterpret_cast<const S4*>(m.u)[e.vbase + i].w;
     reinterpret_cast<S4*>(m.u)[e.vbase + i] = un;
     end_vertex<SReal>(m, e.vbase + i, un, sc);
   }
   if (stat) atomicOr(&s_stat, stat);
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (GROUP && g > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    if (threadIdx.x == 0 && rank != 0 && s_stat)
+      atomicOr(cl.map_shared_rank(&s_stat, 0), s_stat);
+    cl.sync();  // also the last access of another block's shared memory
+  }
+  if (threadIdx.x == 0 && rank == 0) {
     m.iters[env] = it;
     m.status[env] = s_stat | (converged ? 0u : kStatIterCap);
   }
@@ -112,12 +212,12 @@ __global__ void begin_kernel(DevMesh m, const StepParams* __restrict__ pp, LoopC
     ctl->status = 0u;
   }
   if (i < e.nv) {
-    const real4<Real> un = begin_vertex<Real>(m, e.vbase + i, i < e.nact, sc);
+    const real4<Real> un = begin_vertex<Real>(m, e.vbase + i, i < e.nact, sc, true);
     reinterpret_cast<real4<Real>*>(m.u)[e.vbase + i] = un;
   }
 }
 
-template <typename Real, typename SReal, int TPV, int MAT>
+template <typename Real, typename SReal, int TPV, int MAT, int FMT>
 __global__ void __launch_bounds__(256) color_kernel(DevMesh m, int color,
                                                     const StepParams* __restrict__ pp,
                                                     LoopControl* ctl) {
@@ -129,9 +229,9 @@ __global__ void __launch_bounds__(256) color_kernel(DevMesh m, int color,
   const int q = ci.chunk_begin + blockIdx.x * (blockDim.x >> 5) + warp;
   unsigned long long cmax = 0ull;
   unsigned stat = 0u;
+  const GlobalState<SReal> state{reinterpret_cast<S4*>(m.u)};
   if (q < ci.chunk_end)
-    process_chunk<Real, SReal, TPV, MAT, false>(m, 0, ci, q, lane, reinterpret_cast<S4*>(m.u),
-                                                sc, cmax, stat);
+    process_chunk<Real, SReal, TPV, MAT, FMT>(m, 0, ci, q, lane, state, sc, cmax, stat);
   cmax = warp_max_u64(cmax);
   const unsigned st = __reduce_or_sync(0xffffffffu, stat);
   if (lane == 0) {
@@ -225,75 +325,102 @@ namespace {
 // opt-in limit is 227 KB per block including the kernel's static shared memory
 constexpr int kMaxSmem = 227 * 1024 - 2048;
 
-template <typename Real, typename SReal, int TPV, int MAT>
-cudaError_t env_launch_t(int threads, const DevMesh& m, const StepParams& p, const double* tol,
-                         int n_env, size_t smem, cudaStream_t s) {
-  static int configured_device = -1;  // the attribute is per device
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
+cudaError_t configure_env_kernel() {
+  static int configured_device = -1;  // the attributes are per device
   int dev = 0;
   cudaGetDevice(&dev);
-  if (configured_device != dev) {
-    cudaError_t e = cudaFuncSetAttribute(env_step_kernel<Real, SReal, TPV, MAT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (configured_device == dev) return cudaSuccess;
+  auto* k = env_step_kernel<Real, SReal, TPV, MAT, FMT, GROUP>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+  if (e == cudaSuccess && GROUP)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e == cudaSuccess) configured_device = dev;
+  return e;
+}
+
+struct EnvLaunch {
+  int threads;
+  const DevMesh& m;
+  const StepParams& p;
+  const double* tol;
+  const int4* work;
+  int n_blocks, cluster;
+  size_t smem;
+  cudaStream_t s;
+  template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+  cudaError_t run() {
+    if (cluster <= 1) {
+      cudaError_t e = configure_env_kernel<Real, SReal, TPV, MAT, FMT, false>();
+      if (e != cudaSuccess) return e;
+      env_step_kernel<Real, SReal, TPV, MAT, FMT, false><<<n_blocks, threads, smem, s>>>(
+          m, p, tol, work);
+      return cudaGetLastError();
+    }
+    cudaError_t e = configure_env_kernel<Real, SReal, TPV, MAT, FMT, true>();
     if (e != cudaSuccess) return e;
-    configured_device = dev;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_blocks);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, env_step_kernel<Real, SReal, TPV, MAT, FMT, true>, m, p, tol,
+                              work);
   }
-  env_step_kernel<Real, SReal, TPV, MAT><<<n_env, threads, smem, s>>>(m, p, tol);
-  return cudaGetLastError();
-}
+};
 
-template <typename Real, typename SReal, int MAT>
-cudaError_t env_launch_m(int tpv, int threads, const DevMesh& m, const StepParams& p,
-                         const double* tol, int n_env, size_t smem, cudaStream_t s) {
-  switch (tpv) {
-    case 1: return env_launch_t<Real, SReal, 1, MAT>(threads, m, p, tol, n_env, smem, s);
-    case 2: return env_launch_t<Real, SReal, 2, MAT>(threads, m, p, tol, n_env, smem, s);
-    case 4: return env_launch_t<Real, SReal, 4, MAT>(threads, m, p, tol, n_env, smem, s);
-    case 8: return env_launch_t<Real, SReal, 8, MAT>(threads, m, p, tol, n_env, smem, s);
-    case 16: return env_launch_t<Real, SReal, 16, MAT>(threads, m, p, tol, n_env, smem, s);
-    case 32: return env_launch_t<Real, SReal, 32, MAT>(threads, m, p, tol, n_env, smem, s);
-    default: return cudaErrorInvalidValue;
+// Resident blocks per SM (cluster = 1) or resident clusters on the device.
+struct EnvOccupancy {
+  int threads;
+  size_t smem;
+  int cluster;
+  int* out;
+  template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+  cudaError_t run() {
+    if (cluster <= 1) {
+      cudaError_t e = configure_env_kernel<Real, SReal, TPV, MAT, FMT, false>();
+      if (e != cudaSuccess) return e;
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          out, env_step_kernel<Real, SReal, TPV, MAT, FMT, false>, threads, smem);
+    }
+    cudaError_t e = configure_env_kernel<Real, SReal, TPV, MAT, FMT, true>();
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster * 64);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaOccupancyMaxActiveClusters(out, env_step_kernel<Real, SReal, TPV, MAT, FMT, true>,
+                                          &cfg);
   }
-}
+};
 
-template <typename Real, typename SReal, int MAT>
-cudaError_t color_launch_m(int tpv, int threads, const DevMesh& m, int color, int n_chunks,
-                           const StepParams* p, LoopControl* ctl, cudaStream_t s) {
-  const int wpb = threads / 32;
-  const int blocks = (n_chunks + wpb - 1) / wpb;
-  if (blocks == 0) return cudaSuccess;
-#define VBD_COLOR(T)                                                                        \
-  color_kernel<Real, SReal, T, MAT><<<blocks, threads, 0, s>>>(m, color, p, ctl);          \
-  break
-  switch (tpv) {
-    case 1: VBD_COLOR(1);
-    case 2: VBD_COLOR(2);
-    case 4: VBD_COLOR(4);
-    case 8: VBD_COLOR(8);
-    case 16: VBD_COLOR(16);
-    case 32: VBD_COLOR(32);
-    default: return cudaErrorInvalidValue;
+struct ColorLaunch {
+  int blocks, threads;
+  const DevMesh& m;
+  int color;
+  const StepParams* p;
+  LoopControl* ctl;
+  cudaStream_t s;
+  template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+  cudaError_t run() {
+    color_kernel<Real, SReal, TPV, MAT, FMT><<<blocks, threads, 0, s>>>(m, color, p, ctl);
+    return cudaGetLastError();
   }
-#undef VBD_COLOR
-  return cudaGetLastError();
-}
-
-template <typename Real, typename SReal>
-cudaError_t env_launch_p(int material, int tpv, int threads, const DevMesh& m,
-                         const StepParams& p, const double* tol, int n_env, size_t smem,
-                         cudaStream_t s) {
-  return material == kSNH
-             ? env_launch_m<Real, SReal, kSNH>(tpv, threads, m, p, tol, n_env, smem, s)
-             : env_launch_m<Real, SReal, kStVK>(tpv, threads, m, p, tol, n_env, smem, s);
-}
-
-template <typename Real, typename SReal>
-cudaError_t color_launch_p(int material, int tpv, int threads, const DevMesh& m, int color,
-                           int n_chunks, const StepParams* p, LoopControl* ctl,
-                           cudaStream_t s) {
-  return material == kSNH
-             ? color_launch_m<Real, SReal, kSNH>(tpv, threads, m, color, n_chunks, p, ctl, s)
-             : color_launch_m<Real, SReal, kStVK>(tpv, threads, m, color, n_chunks, p, ctl, s);
-}
+};
 
 inline int nblk(int n, int t) { return (n + t - 1) / t; }
 }  // namespace
@@ -301,27 +428,28 @@ inline int nblk(int n, int t) { return (n + t - 1) / t; }
 int env_kernel_max_smem() { return kMaxSmem; }
 
 cudaError_t launch_env_step(int prec, int material, int tpv, int threads, const DevMesh& m,
-                            const StepParams& p, const double* tol_env, int n_env,
-                            size_t smem, cudaStream_t s) {
+                            const StepParams& p, const double* tol_env, const int4* work,
+                            int n_blocks, int cluster, size_t smem, cudaStream_t s) {
   if (threads < 32 || threads > 512 || threads % 32) return cudaErrorInvalidValue;
-  switch (prec) {
-    case 0: return env_launch_p<float, float>(material, tpv, threads, m, p, tol_env, n_env, smem, s);
-    case 1: return env_launch_p<float, double>(material, tpv, threads, m, p, tol_env, n_env, smem, s);
-    case 2: return env_launch_p<double, double>(material, tpv, threads, m, p, tol_env, n_env, smem, s);
-    default: return cudaErrorInvalidValue;
-  }
+  if (cluster < 1 || cluster > kMaxGroup || n_blocks % cluster) return cudaErrorInvalidValue;
+  EnvLaunch f{threads, m, p, tol_env, work, n_blocks, cluster, smem, s};
+  return dispatch(prec, material, m.fmt, tpv, f);
+}
+
+cudaError_t env_occupancy(int prec, int material, int fmt, int tpv, int threads, size_t smem,
+                          int cluster, int* out) {
+  EnvOccupancy f{threads, smem, cluster, out};
+  return dispatch(prec, material, fmt, tpv, f);
 }
 
 cudaError_t launch_color(int prec, int material, int tpv, int threads, const DevMesh& m,
                          int color, int n_chunks, const StepParams* p, LoopControl* ctl,
                          cudaStream_t s) {
   if (threads != 256) return cudaErrorInvalidValue;  // color_kernel reduces over 8 warps
-  switch (prec) {
-    case 0: return color_launch_p<float, float>(material, tpv, threads, m, color, n_chunks, p, ctl, s);
-    case 1: return color_launch_p<float, double>(material, tpv, threads, m, color, n_chunks, p, ctl, s);
-    case 2: return color_launch_p<double, double>(material, tpv, threads, m, color, n_chunks, p, ctl, s);
-    default: return cudaErrorInvalidValue;
-  }
+  const int blocks = (n_chunks + 7) / 8;
+  if (blocks == 0) return cudaSuccess;
+  ColorLaunch f{blocks, threads, m, color, p, ctl, s};
+  return dispatch(prec, material, m.fmt, tpv, f);
 }
 
 cudaError_t launch_begin(bool state64, const DevMesh& m, const StepParams* p, LoopControl* ctl,

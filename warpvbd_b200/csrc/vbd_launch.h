@@ -12,10 +12,17 @@ namespace vbd {
 // Largest dynamic shared memory a block-mode step may use (bytes).
 int env_kernel_max_smem();
 
-// Block mode: one thread block per environment runs begin, all sweeps and end.
+// Block mode: work[b] = (environment, rank, group size) for block b; an
+// environment runs begin, all sweeps and end on one block, or on all blocks
+// of one cluster (group size = cluster).  n_blocks must be a multiple of
+// cluster (padding blocks carry environment -1).
 cudaError_t launch_env_step(int prec, int material, int tpv, int threads, const DevMesh& m,
-                            const StepParams& p, const double* tol_env, int n_env,
-                            size_t smem_bytes, cudaStream_t s);
+                            const StepParams& p, const double* tol_env, const int4* work,
+                            int n_blocks, int cluster, size_t smem_bytes, cudaStream_t s);
+// Resident env_step blocks per SM (cluster == 1) or resident clusters on the
+// device (cluster > 1) for this launch shape.
+cudaError_t env_occupancy(int prec, int material, int fmt, int tpv, int threads, size_t smem,
+                          int cluster, int* out);
 
 // Grid mode building blocks (single environment).
 cudaError_t launch_begin(bool state64, const DevMesh& m, const StepParams* p, LoopControl* ctl,

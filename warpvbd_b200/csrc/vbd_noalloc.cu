@@ -45,7 +45,7 @@ int noalloc_max_partials() { return kNoAllocMaxPartials; }
 
 // Colour sweep writing its block maximum to partial[blockIdx.x] instead of an
 // atomic on the solver's loop-control word.
-template <typename Real, typename SReal, int TPV, int MAT>
+template <typename Real, typename SReal, int TPV, int MAT, int FMT>
 __global__ void __launch_bounds__(256) noalloc_color_kernel(DevMesh m, int color,
                                                             const StepParams* __restrict__ pp,
                                                             LoopControl* ctl,
@@ -58,9 +58,9 @@ __global__ void __launch_bounds__(256) noalloc_color_kernel(DevMesh m, int color
   const int q = ci.chunk_begin + blockIdx.x * (blockDim.x >> 5) + warp;
   unsigned long long cmax = 0ull;
   unsigned stat = 0u;
+  const GlobalState<SReal> state{reinterpret_cast<S4*>(m.u)};
   if (q < ci.chunk_end)
-    process_chunk<Real, SReal, TPV, MAT, false>(m, 0, ci, q, lane, reinterpret_cast<S4*>(m.u),
-                                                sc, cmax, stat);
+    process_chunk<Real, SReal, TPV, MAT, FMT>(m, 0, ci, q, lane, state, sc, cmax, stat);
   cmax = warp_max_u64(cmax);
   const unsigned st = __reduce_or_sync(0xffffffffu, stat);
   if (lane == 0) {
@@ -94,48 +94,30 @@ __global__ void __launch_bounds__(256) noalloc_reduce_kernel(const unsigned long
 
 namespace {
 
-template <typename Real, typename SReal, int MAT>
-cudaError_t noalloc_color_launch(int tpv, const DevMesh& m, int color, int blocks,
-                                 const StepParams* p, LoopControl* ctl,
-                                 unsigned long long* partial, cudaStream_t s) {
-  if (blocks == 0) return cudaSuccess;
-#define VBD_NA(T)                                                                           \
-  noalloc_color_kernel<Real, SReal, T, MAT><<<blocks, 256, 0, s>>>(m, color, p, ctl, partial); \
-  break
-  switch (tpv) {
-    case 1: VBD_NA(1);
-    case 2: VBD_NA(2);
-    case 4: VBD_NA(4);
-    case 8: VBD_NA(8);
-    case 16: VBD_NA(16);
-    case 32: VBD_NA(32);
-    default: return cudaErrorInvalidValue;
+struct NoAllocColorLaunch {
+  int blocks;
+  const DevMesh& m;
+  int color;
+  const StepParams* p;
+  LoopControl* ctl;
+  unsigned long long* partial;
+  cudaStream_t s;
+  template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+  cudaError_t run() {
+    noalloc_color_kernel<Real, SReal, TPV, MAT, FMT><<<blocks, 256, 0, s>>>(m, color, p, ctl,
+                                                                             partial);
+    return cudaGetLastError();
   }
-#undef VBD_NA
-  return cudaGetLastError();
-}
-
-template <typename Real, typename SReal>
-cudaError_t noalloc_color_p(int material, int tpv, const DevMesh& m, int color, int blocks,
-                            const StepParams* p, LoopControl* ctl, unsigned long long* partial,
-                            cudaStream_t s) {
-  return material == kSNH
-             ? noalloc_color_launch<Real, SReal, kSNH>(tpv, m, color, blocks, p, ctl, partial, s)
-             : noalloc_color_launch<Real, SReal, kStVK>(tpv, m, color, blocks, p, ctl, partial,
-                                                        s);
-}
+};
 
 }  // namespace
 
 cudaError_t launch_noalloc_color(int prec, int material, int tpv, const DevMesh& m, int color,
                                  int blocks, const StepParams* p, LoopControl* ctl,
                                  unsigned long long* partial, cudaStream_t s) {
-  switch (prec) {
-    case 0: return noalloc_color_p<float, float>(material, tpv, m, color, blocks, p, ctl, partial, s);
-    case 1: return noalloc_color_p<float, double>(material, tpv, m, color, blocks, p, ctl, partial, s);
-    case 2: return noalloc_color_p<double, double>(material, tpv, m, color, blocks, p, ctl, partial, s);
-    default: return cudaErrorInvalidValue;
-  }
+  if (blocks == 0) return cudaSuccess;
+  NoAllocColorLaunch f{blocks, m, color, p, ctl, partial, s};
+  return dispatch(prec, material, m.fmt, tpv, f);
 }
 
 cudaError_t launch_noalloc_reduce(const unsigned long long* partial, int n, LoopControl* ctl,

@@ -104,6 +104,8 @@ class VBDSolver:
                  "fp32" (everything fp32) or "fp64" (everything fp64)
       mode       "auto", "block", "graph" or "hostloop" (see include/vbd_b200.h)
       tpv, block_threads   launch shape (0 = automatic)
+      cluster    block mode: spread the mesh over this many thread blocks of one
+                 cluster (1, 2, 4, 8, 16; 0 = automatic)
       coloring   per-vertex colours to use instead of the greedy colouring
       strict_spd raise instead of taking the guarded step on a non-SPD block
       allow_high_valence  lift the reference's 32 incident-tets limit
@@ -112,7 +114,7 @@ class VBDSolver:
     def __init__(self, initial_positions, elements, densities, youngs_modulus, poissons_ratio,
                  damping_coefficient=1.0, active_mask=None, gravity=(0.0, 0.0, -9.81),
                  dx_tol=1e-9, max_iter=100, device="cuda", *, material="snh",
-                 precision="mixed", mode="auto", tpv=0, block_threads=0, coloring=None,
+                 precision="mixed", mode="auto", tpv=0, block_threads=0, cluster=0, coloring=None,
                  strict_spd=False, allow_high_valence=False, verbose=False):
         L = _lib.load()
         X = _lib.f64(_host(initial_positions), (-1, 3))
@@ -136,6 +138,7 @@ class VBDSolver:
         flags |= _lib.MODES[mode]
         if strict_spd:
             flags |= _lib.STRICT_SPD
+        flags |= int(cluster) << _lib.CLUSTER_SHIFT
         self.device = device
         self._dev = _device_index(device)
         h = ctypes.c_void_p()
