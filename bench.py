@@ -12,6 +12,8 @@ colour sweeps until max|dx_x+dx_y+dx_z| < tol, velocity update).
 value = simulated environment-seconds per wall second, summed over ranks
 (each rank steps its own copy of the batch: weak scaling, no collective on
 the data path).  Other workloads: cantilever20/40/80/160/320, massspring.
+The batched workload is also timed with the learned warm start
+(``warm_start_batched``; ``--warmstart on`` makes it the headline).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
   python bench.py --impl reference ...   # FP64 CPU oracle on the host cores
@@ -198,14 +200,27 @@ def run_reference(args, envs, desc, batched):
     print(json.dumps(line), flush=True)
 
 
-def make_solver(envs, batched, local, mode="auto"):
+def make_solver(envs, batched, local, mode="auto", warm=None):
     if batched:
         from warpvbd_b200 import BatchedVBDSolver
-        return BatchedVBDSolver(envs, dx_tol=TOL, max_iter=MAX_ITER, device=f"cuda:{local}")
-    from warpvbd_b200 import VBDSolver
-    s = envs[0]
-    return VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL, max_iter=MAX_ITER,
-                     device=f"cuda:{local}", mode=mode)
+        sol = BatchedVBDSolver(envs, dx_tol=TOL, max_iter=MAX_ITER, device=f"cuda:{local}")
+    else:
+        from warpvbd_b200 import VBDSolver
+        s = envs[0]
+        sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL,
+                        max_iter=MAX_ITER, device=f"cuda:{local}", mode=mode)
+    if warm is not None:
+        sol.set_warmstart(warm)
+    return sol
+
+
+def warm_params(args, batched):
+    """Trained warm-start model (committed file) for the batched workloads
+    with --warmstart on."""
+    if args.warmstart == "off" or not batched:
+        return None
+    from warpvbd_b200 import warmstart
+    return warmstart.load()
 
 
 def step_async(sol, batched):
@@ -245,7 +260,8 @@ def run_ours(args, envs, desc, batched):
     world, rank, local = dist_init()
     torch.cuda.set_device(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-    sol = make_solver(envs, batched, local, args.mode)
+    warm = warm_params(args, batched)
+    sol = make_solver(envs, batched, local, args.mode, warm)
     info = sol.info()
     if world > 1:
         torch.distributed.barrier()
@@ -283,12 +299,15 @@ def run_ours(args, envs, desc, batched):
     slots = np.array([p[2] for p in per_env])
     solved = np.array([p[1] for p in per_env])
     mode = {0x100: "block", 0x200: "graph", 0x300: "hostloop"}[info["mode"]]
-    alg_bytes = float((iters * b_sweep[None, :]).sum())
+    # sweeps, plus the two energy passes over every slot when the warm start
+    # compares the prediction with the inertia guess
+    passes = iters + (2 if warm is not None else 0)
+    alg_bytes = float((passes * b_sweep[None, :]).sum())
     achieved = alg_bytes / (total_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     kernel = "env_step_kernel" if mode == "block" else "color_kernel"
     tps = profile_traffic_per_slot(kernel, args.workload)
-    traffic = None if tps is None else tps * float((iters * slots[None, :]).sum()) / args.steps
+    traffic = None if tps is None else tps * float((passes * slots[None, :]).sum()) / args.steps
     launches = args.steps if mode == "block" else int(
         args.steps * 2 + iters.sum() * (info["n_colors"] + 1))
     line = {"metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s",
@@ -300,6 +319,7 @@ def run_ours(args, envs, desc, batched):
                        "max_iter": MAX_ITER, "mode": mode, "tpv": info["tpv"],
                        "block_threads": info["block_threads"],
                        "parallelism": f"replicas x{world}",
+                       "warm_start": warm is not None,
                        "l2": "256 MiB written between timed steps"},
             "iters_per_step": {"mean": float(iters.mean()), "max": int(iters.max()),
                                "min": int(iters.min())},
@@ -323,6 +343,42 @@ def run_ours(args, envs, desc, batched):
             "sample": f"{k} whole steps of {len(sample)} environment(s) "
                       + ("concatenated into one mesh " if batched else "")
                       + f"({el:.1f} s), FP64 C oracle, OpenMP {n} threads"}
+    if batched and not args.no_secondary:
+        # the same batch with the learned warm start toggled (same timing
+        # method); every rank takes this path, so the collectives match
+        from warpvbd_b200 import warmstart
+        sol.close()
+        other = None if warm is not None else warmstart.load()
+        ps = make_solver(envs, batched, local, warm=other)
+        pms, pit, _ = timed_steps(ps, batched, args.steps, args.warmup, local, flush)
+        pt = float(pms.sum())
+        if world > 1:
+            t = torch.tensor([pt], device=f"cuda:{local}")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            pt = float(t.item())
+        ppass = pit + (2 if other is not None else 0)
+        pbytes = float((ppass * b_sweep[None, :]).sum())
+        pv = world * n_env * args.steps * DT / (pt * 1e-3)
+        key = "warm_start_batched" if other is not None else "plain_batched"
+        line[key] = {
+            "value": pv, "ms_per_step": pt / args.steps,
+            "iters_per_step": {"mean": float(pit.mean()), "max": int(pit.max())},
+            "roofline_frac": pbytes / (pt * 1e-3) / 1e9 / peak}
+        warm_v, plain_v = (pv, value) if other is not None else (value, pv)
+        line["warm_start_speedup_vs_plain_batched"] = warm_v / plain_v
+        ps.close()
+    if rank == 0 and world == 1 and batched and not args.no_secondary:
+        # plain VBD one environment at a time (single-environment solver), on a
+        # sample of the batch: what the batch costs without batching
+        t_seq, n_seq = 0.0, 0
+        for env in envs[:16]:
+            es = make_solver([env], False, local)
+            ems, _, _ = timed_steps(es, False, 5, 3, local, flush)
+            t_seq += float(ems.sum()) * 1e-3
+            n_seq += 5
+            es.close()
+        line["plain_one_env_at_a_time"] = {
+            "value": n_seq * DT / t_seq, "sample": "16 environments x 5 steps each"}
     if rank == 0 and world == 1 and batched and not args.no_secondary:
         # the plain single-mesh solver on the 160x16x16 cantilever
         cant = scenes.cantilever(160)
@@ -359,6 +415,9 @@ def main():
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--warmstart", default="off", choices=["off", "on"],
+                    help="headline batched run starts steps from the trained network (on); "
+                         "the other setting is timed as a secondary figure")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     envs, desc, batched = make_workload(args.workload)

@@ -166,6 +166,51 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info);
 /* The CUDA stream (cudaStream_t) all of the solver's work is enqueued on. */
 void* vbd_get_stream(vbd_solver* s);
 
+/* ---- learned warm start (not in the reference) ------------------------------
+ * A per-vertex MLP (22 inputs -> 64 SiLU -> 64 SiLU -> 3) predicts each
+ * step's converged-minus-inertia correction (scale-free: relative to the
+ * vertex's motion scale); the step starts from the
+ * prediction when it lowers the incremental potential and from the inertia
+ * guess otherwise, then iterates to the same tolerance.  Parameters are fp32
+ * in the order W1[64][22] b1[64] W2[64][64] b2[64] W3[3][64] b3[3]; inference
+ * runs with bf16 weights.  Feature rows hold vbd_ws_feature_width() floats in
+ * the solver's internal vertex order (element 23 = 1 for solved vertices).
+ * Pointers named "device" below are CUDA device pointers. */
+int vbd_ws_param_count(void);
+int vbd_ws_feature_width(void);
+/* params: host fp32 [vbd_ws_param_count()] to enable, NULL to disable
+ * (block mode only).  The network acts on normalised features and predicts
+ * normalised targets; norm (host fp32 [50], NULL = identity) holds the
+ * inputs' mean[22] and 1/std[22], then the targets' std[3] and mean[3]. */
+int vbd_set_warmstart(vbd_solver* s, const float* params, const float* norm);
+/* Features of the coming step of length dt at the current state, into device
+ * [n_vertices][feature_width]. */
+int vbd_ws_features(vbd_solver* s, double dt, float* features);
+/* After a step: the correction it converged to, (x_new - inertia guess) / h,
+ * into device [n_vertices][3] (zero rows where features flag 0). */
+int vbd_ws_targets(vbd_solver* s, const float* features, float* targets);
+/* The model's predicted corrections for given features (the inference the
+ * step runs), into device [n_vertices][4] (xyz in metres, w = 1 where
+ * predicted). */
+int vbd_ws_predict(vbd_solver* s, const float* features, float* predictions);
+/* Per-environment status bits of the last step: 1 non-finite, 2 guarded
+ * step taken, 4 max_iter reached, 16 started from the learned prediction. */
+int vbd_get_env_status(vbd_solver* s, uint32_t* status_out);
+/* One minibatch of training on device data: rows idx[0..batch) (NULL = the
+ * first batch rows) of X [N][feature_width] and Y [N][3]; writes the loss
+ * gradient with respect to params into grad and adds sum of squared errors to
+ * *loss (device double, may be NULL).  scratch: device floats, at least
+ * batch * (4 * 64 + 3).  Enqueued on `stream`. */
+int vbd_mlp_train_batch(const float* X, const float* Y, const int32_t* idx, int batch,
+                        const float* params, float* grad, float* scratch, double* loss,
+                        void* stream);
+/* fp32 forward pass: out [n][3] (device); scratch: at least n * 128 floats. */
+int vbd_mlp_forward(const float* X, int n, const float* params, float* out, float* scratch,
+                    void* stream);
+/* Adam update of n parameters, step t >= 1 (device arrays). */
+int vbd_mlp_adam(float* params, const float* grad, float* m, float* v, int n, float lr,
+                 float beta1, float beta2, float eps, int t, void* stream);
+
 /* vbd_step for callers that may not allocate GPU memory while they step: an
  * application that commits its whole device-memory budget at start-up, or a
  * real-time loop whose per-step code may not call an allocator.  Create the

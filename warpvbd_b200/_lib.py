@@ -89,6 +89,20 @@ SIGNATURES = {
     "vbd_get_stream": (_vp, [_vp]),
     "vbd_step_noalloc": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                         _ip]),
+    "vbd_ws_param_count": (ctypes.c_int, []),
+    "vbd_ws_feature_width": (ctypes.c_int, []),
+    "vbd_set_warmstart": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_float),
+                                         ctypes.POINTER(ctypes.c_float)]),
+    "vbd_ws_features": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
+    "vbd_ws_targets": (ctypes.c_int, [_vp, _vp, _vp]),
+    "vbd_ws_predict": (ctypes.c_int, [_vp, _vp, _vp]),
+    "vbd_get_env_status": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "vbd_mlp_train_batch": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                           _vp]),
+    "vbd_mlp_forward": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "vbd_mlp_adam": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                    _vp]),
 }
 
 _lib = None

@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .vbd_solver import _host, _device_index
+from .vbd_solver import _host, _device_index, _set_warmstart, _ws_features, _ws_targets
 
 
 class BatchedVBDSolver:
@@ -136,6 +136,31 @@ class BatchedVBDSolver:
 
     def reset(self):
         _lib.check(_lib.load().vbd_reset(self._h))
+
+    # ---- learned warm start (see warpvbd_b200.warmstart) --------------------
+    def set_warmstart(self, params):
+        return _set_warmstart(self._h, params)
+
+    def ws_features(self, dt, out=None):
+        return _ws_features(self._h, self.n_vertices, dt, out)
+
+    def ws_targets(self, features, out=None):
+        return _ws_targets(self._h, self.n_vertices, features, out)
+
+    def ws_predict(self, features, out=None):
+        import torch
+        if out is None:
+            out = torch.empty((self.n_vertices, 4), device=features.device)
+        _lib.check(_lib.load().vbd_ws_predict(self._h, ctypes.c_void_p(features.data_ptr()),
+                                              ctypes.c_void_p(out.data_ptr())), "vbd_ws_predict")
+        return out
+
+    def env_status(self):
+        """Per-environment status bits of the last step (16 = warm start used)."""
+        out = np.zeros(self.n_env, np.uint32)
+        _lib.check(_lib.load().vbd_get_env_status(
+            self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))))
+        return out
 
     def close(self):
         h = getattr(self, "_h", None)

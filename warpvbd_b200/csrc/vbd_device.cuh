@@ -346,6 +346,105 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
   }
 }
 
+// ---------------------------------------------------------------------------
+// Incremental potential.  Per slot: the slot's share (q2.w) of the tet's
+// strain energy V psi(F), with the same G as slot_accumulate:
+//   SNH   psi = mu'/2 (Ic-3) - mu'/2 ln((Ic+1)/4) + lambda'/2 (J-alpha)^2
+//   StVK  psi = mu E:E + lambda/2 tr(E)^2
+// (the SNH form differs from mu'/2 (Ic-3) - mu'/2 ln(Ic+1) + ... by a
+// constant, and its F-derivative is the P of slot_accumulate).  Used only to
+// compare two configurations, so constants cancel.
+// ---------------------------------------------------------------------------
+template <typename Real, int MAT>
+__device__ __forceinline__ Real slot_energy(Real d0x, Real d0y, Real d0z, Real d1x, Real d1y,
+                                            Real d1z, Real d2x, Real d2y, Real d2z,
+                                            const real4<Real>& q0, const real4<Real>& q1,
+                                            const real4<Real>& q2) {
+  const Real G00 = d0x * q0.x + d1x * q1.x + d2x * q2.x;
+  const Real G01 = d0x * q0.y + d1x * q1.y + d2x * q2.y;
+  const Real G02 = d0x * q0.z + d1x * q1.z + d2x * q2.z;
+  const Real G10 = d0y * q0.x + d1y * q1.x + d2y * q2.x;
+  const Real G11 = d0y * q0.y + d1y * q1.y + d2y * q2.y;
+  const Real G12 = d0y * q0.z + d1y * q1.z + d2y * q2.z;
+  const Real G20 = d0z * q0.x + d1z * q1.x + d2z * q2.x;
+  const Real G21 = d0z * q0.y + d1z * q1.y + d2z * q2.y;
+  const Real G22 = d0z * q0.z + d1z * q1.z + d2z * q2.z;
+  const Real p0 = q0.w, p1 = q1.w, w = q2.w;
+  const Real t = G00 + G11 + G22;
+  Real psi;
+  if (MAT == kSNH) {
+    const Real c00 = G11 * G22 - G12 * G21, c01 = G12 * G20 - G10 * G22,
+               c02 = G10 * G21 - G11 * G20;
+    const Real detG = G00 * c00 + G01 * c01 + G02 * c02;
+    const Real trG2 =
+        G00 * G00 + G11 * G11 + G22 * G22 + Real(2) * (G01 * G10 + G02 * G20 + G12 * G21);
+    const Real nG2 = G00 * G00 + G01 * G01 + G02 * G02 + G10 * G10 + G11 * G11 + G12 * G12 +
+                     G20 * G20 + G21 * G21 + G22 * G22;
+    const Real Jm1 = t + Real(0.5) * (t * t - trG2) + detG;
+    const Real Icm3 = Real(2) * t + nG2;
+    const Real am1 = Real(0.75) * p0 / p1;  // alpha - 1 = 3/4 mu' / lambda'
+    const Real r = Jm1 - am1;
+    psi = Real(0.5) * p0 * (Icm3 - log1p(Real(0.25) * Icm3)) + Real(0.5) * p1 * r * r;
+  } else {
+    const Real E00 = G00 + Real(0.5) * (G00 * G00 + G10 * G10 + G20 * G20);
+    const Real E11 = G11 + Real(0.5) * (G01 * G01 + G11 * G11 + G21 * G21);
+    const Real E22 = G22 + Real(0.5) * (G02 * G02 + G12 * G12 + G22 * G22);
+    const Real E01 = Real(0.5) * (G01 + G10 + G00 * G01 + G10 * G11 + G20 * G21);
+    const Real E02 = Real(0.5) * (G02 + G20 + G00 * G02 + G10 * G12 + G20 * G22);
+    const Real E12 = Real(0.5) * (G12 + G21 + G01 * G02 + G11 * G12 + G21 * G22);
+    const Real trE = E00 + E11 + E22;
+    const Real EE = E00 * E00 + E11 * E11 + E22 * E22 +
+                    Real(2) * (E01 * E01 + E02 * E02 + E12 * E12);
+    psi = p0 * EE + Real(0.5) * p1 * trE * trE;
+  }
+  return w * psi;
+}
+
+// Energy of one chunk's vertices at the state `st`: strain-energy shares of
+// their slots plus, with inertia, m/(2 dt^2) |u - ut|^2 per vertex.
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
+__device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, const ColorInfo& ci,
+                                               int q, int lane, const State& st,
+                                               const StepConst& sc, bool inertia) {
+  using R4 = real4<Real>;
+  using S4 = real4<SReal>;
+  constexpr int CPW = 32 / TPV;
+  const int vi = lane / TPV, sub = lane % TPV;
+  const int gv = ci.vbegin + (q - ci.chunk_begin) * CPW + vi;
+  const bool valid = gv < ci.vend;
+  const int lv = gv - vbase;
+  const ChunkInfo ch = m.chunk[q];
+  int k = 0;
+  S4 uo;
+  uo.x = uo.y = uo.z = uo.w = SReal(0);
+  if (valid) {
+    k = __ldg(m.valence + gv);
+    uo = st.load(lv);
+  }
+  double acc = 0.0;
+  const R4* tab = reinterpret_cast<const R4*>(m.rec_tab);
+  const size_t base = (size_t)ch.block * 32 + lane;
+  for (int s = 0; s < ch.steps; ++s) {
+    if (s * TPV + sub < k) {
+      const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
+      const R4* t = tab + 3 * (size_t)id.w;
+      const S4 a = st.load(id.x);
+      const S4 b = st.load(id.y);
+      const S4 c = st.load(id.z);
+      acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                                           Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                                           Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
+                                           ldg4(t), ldg4(t + 1), ldg4(t + 2)));
+    }
+  }
+  if (inertia && valid && sub == 0) {
+    const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
+    const double dx = double(uo.x - tt.x), dy = double(uo.y - tt.y), dz = double(uo.z - tt.z);
+    acc += 0.5 * double(tt.w) * sc.inv_dt2 * (dx * dx + dy * dy + dz * dz);
+  }
+  return acc;
+}
+
 // Inertia target and initial guess (position_initialization,
 // vbd_solver.py:277-292): ut = u + dt v + dt^2 g (w keeps the lumped mass),
 // up = u (written when write_back), and active vertices start from ut.

@@ -23,6 +23,7 @@
 #include "vbd_internal.h"
 #include "vbd_launch.h"
 #include "vbd_noalloc.h"
+#include "vbd_warmstart.h"
 
 using namespace vbd;
 
@@ -98,7 +99,8 @@ int greedy_coloring(const int32_t* tets, int T, int nv, int32_t* col) {
 struct TetData {
   std::vector<double> b;  // [T][4][3] shape-function gradients
   std::vector<double> p;  // [T][3] (V*mu, V*lambda, alpha)
-  std::vector<double> mass;
+  std::vector<double> mass, vol;
+  const double *E = nullptr, *nu = nullptr, *rho = nullptr;  // caller's per-tet arrays
 };
 
 int build_tet_data(const double* X, const int32_t* tets, int T, const double* rho,
@@ -106,6 +108,10 @@ int build_tet_data(const double* X, const int32_t* tets, int T, const double* rh
   td.b.assign((size_t)T * 12, 0.0);
   td.p.assign((size_t)T * 3, 0.0);
   td.mass.assign(T, 0.0);
+  td.vol.assign(T, 0.0);
+  td.E = E;
+  td.nu = nu;
+  td.rho = rho;
   for (int t = 0; t < T; ++t) {
     const int32_t* e = tets + 4 * (size_t)t;
     double D[9];
@@ -132,6 +138,7 @@ int build_tet_data(const double* X, const int32_t* tets, int T, const double* rh
     for (int c = 0; c < 3; ++c) b[9 + c] = -(I[c] + I[3 + c] + I[6 + c]);
     const double vol = std::fabs(det) / 6.0;
     td.mass[t] = rho[t] * vol;
+    td.vol[t] = vol;
     const double mu = E[t] / (2.0 * (1.0 + nu[t]));
     const double lam = (E[t] * nu[t]) / ((1.0 + nu[t]) * (1.0 - 2.0 * nu[t]));
     double* p = &td.p[(size_t)t * 3];
@@ -199,6 +206,8 @@ struct Layout {
   RecordTable table;
   std::vector<int> valence;     // new id
   std::vector<double> mass;     // new id
+  std::vector<float> wstat;     // new id, 4 per vertex: warm-start vertex constants
+  std::vector<int2> chunk_owner;  // (colour index, environment) per chunk
   std::vector<int> new_of_old;
   std::vector<int32_t> table0;  // env 0 colour table (original ids)
   int table_colors = 0, table_max_group = 0;
@@ -215,6 +224,7 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
   L.new_of_old.assign(V, -1);
   L.valence.assign(V, 0);
   L.mass.assign(V, 0.0);
+  L.wstat.assign(4 * (size_t)V, 0.0f);
   int block_count = 0;
   for (int e = 0; e < n_env; ++e) {
     const int vo = voff[e], vn = voff[e + 1] - voff[e];
@@ -335,11 +345,35 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
     for (int v = 0; v < vn; ++v) {
       const int gnew = vo + new_local[v];
       L.new_of_old[vo + v] = gnew;
-      L.valence[gnew] = off[v + 1] - off[v];
-      double m = 0.0;
-      for (int s = off[v]; s < off[v + 1]; ++s) m += td.mass[to + inc[s]] / 4.0;
+      const int k = off[v + 1] - off[v];
+      L.valence[gnew] = k;
+      double m = 0.0, hs = 0.0, logE = 0.0, rho = 0.0, nu = 0.0;
+      for (int s = off[v]; s < off[v + 1]; ++s) {
+        const int t = to + inc[s];
+        m += td.mass[t] / 4.0;
+        hs += std::cbrt(6.0 * td.vol[t]);
+        logE += std::log10(td.E[t]);
+        rho += td.rho[t];
+        nu += td.nu[t];
+      }
       L.mass[gnew] = m;
+      // warm-start vertex constants: local length scale h (mean cube root of
+      // 6 V over the incident tets), log10(E / (rho h^2)), nu, valence / 20
+      float* w4 = &L.wstat[4 * (size_t)gnew];
+      if (k > 0) {
+        const double h = hs / k;
+        w4[0] = (float)h;
+        w4[1] = (float)(logE / k - std::log10(rho / k * h * h));
+        w4[2] = (float)(nu / k);
+        w4[3] = (float)(k / 20.0);
+      } else {
+        w4[0] = 1.0f;
+        w4[1] = w4[2] = w4[3] = 0.0f;
+      }
     }
+    for (int c = ei.cbase; c < ei.cbase + ei.ncolors; ++c)
+      for (int q = L.color[c].chunk_begin; q < L.color[c].chunk_end; ++q)
+        L.chunk_owner.push_back(make_int2(c, e));
     // slot records: (n0, n1, n2, record id) per slot, the record values in a
     // table shared by every slot with the same values in the solver precision
     L.rec_idx.resize((size_t)block_count * 32, make_int4(0, 0, 0, 0));
@@ -365,8 +399,9 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
             double val[12];
             const double* bt = &td.b[(size_t)t * 12];
             const double* pt = &td.p[(size_t)t * 3];
-            int n = 0;
+            int n = 0, solved_in_tet = 0;
             for (int qq = 0; qq < 4; ++qq) {
+              if (new_local[tets[4 * (size_t)t + qq] - vo] < ei.nsolved) ++solved_in_tet;
               if (qq == a) continue;
               ids[n] = new_local[tets[4 * (size_t)t + qq] - vo];
               val[4 * n + 0] = bt[qq * 3 + 0];
@@ -375,6 +410,10 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
               val[4 * n + 3] = pt[n];
               ++n;
             }
+            // 4th value of the last plane: this slot's share of the tet's
+            // strain energy, so that summing over slots counts every tet with
+            // a solved vertex once (incremental-potential evaluation)
+            val[11] = 1.0 / solved_in_tet;
             const int rid = L.table.insert(val);
             L.rec_idx[blk * 32 + lane] = make_int4(ids[0], ids[1], ids[2], rid);
             L.n_slots++;
@@ -421,8 +460,22 @@ struct vbd_solver {
   bool replan = false;       // re-plan from the measured sweep counts after each step
   int capacity_blocks = 0;   // resident blocks on the device for this launch shape
   std::vector<double> env_work;  // incident slots per environment
+  // sweeps per environment for the plan: max(last step, 0.9 x previous
+  // estimate), so an environment whose sweep count jumps between steps keeps
+  // its share of the device
+  std::vector<double> env_sweeps;
   std::vector<int4> work;
   DevBuf<int4> d_work;
+  // learned warm start
+  DevBuf<float4> d_wstat;
+  DevBuf<int2> d_chunk_owner;
+  DevBuf<float> d_feat;           // [V][24], allocated on first use
+  DevBuf<float4> d_pred;          // [V]
+  DevBuf<unsigned char> d_wbf;    // bf16 network parameters
+  DevBuf<float> d_wparams;        // fp32 staging for the conversion
+  DevBuf<float> d_wnorm;          // input / target normalisation (50 floats)
+  bool warm = false;
+  bool ws_history = false;        // the previous step's inertia target is in ut
   // pinned host
   int* h_iters = nullptr;
   unsigned* h_status = nullptr;
@@ -445,6 +498,9 @@ struct vbd_solver {
     m.rec_idx16 = d_rec_idx16.p;
     m.rec_tab = d_rec_tab.p;
     m.fmt = fmt;
+    m.wstat = d_wstat.p;
+    m.chunk_owner = d_chunk_owner.p;
+    m.ws_pred = warm ? d_pred.p : nullptr;
     m.valence = d_valence.p;
     m.u = d_u.p;
     m.ut = d_ut.p;
@@ -486,6 +542,13 @@ void free_solver(vbd_solver* s) {
   s->d_io.release();
   s->d_tol.release();
   s->d_work.release();
+  s->d_wstat.release();
+  s->d_chunk_owner.release();
+  s->d_feat.release();
+  s->d_pred.release();
+  s->d_wbf.release();
+  s->d_wparams.release();
+  s->d_wnorm.release();
   s->d_params.release();
   s->d_ctl.release();
   if (s->h_iters) cudaFreeHost(s->h_iters);
@@ -520,7 +583,10 @@ struct DeviceGuard {
 void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work) {
   const int n = s->n_env, C = s->cluster;
   std::vector<double> w(n);
-  for (int e = 0; e < n; ++e) w[e] = s->env_work[e] * std::max(1, iters ? iters[e] : 1);
+  for (int e = 0; e < n; ++e) {
+    const double sw = (size_t)e < s->env_sweeps.size() ? s->env_sweeps[e] : 1.0;
+    w[e] = s->env_work[e] * std::max(1.0, iters ? std::max((double)iters[e], sw) : sw);
+  }
   std::vector<int> order(n);
   for (int e = 0; e < n; ++e) order[e] = e;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
@@ -745,6 +811,15 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   }
   if (!err && bad(s->d_valence.upload(L.valence, st), "valence")) err = 1;
   if (!err && bad(s->d_map.upload(L.new_of_old, st), "map")) err = 1;
+  if (!err) {
+    std::vector<float4> ws(V);
+    for (int i = 0; i < V; ++i)
+      ws[i] = make_float4(L.wstat[4 * (size_t)i], L.wstat[4 * (size_t)i + 1],
+                          L.wstat[4 * (size_t)i + 2], L.wstat[4 * (size_t)i + 3]);
+    if (bad(s->d_wstat.upload(ws, st), "wstat")) err = 1;
+    if (!err && bad(s->d_chunk_owner.upload(L.chunk_owner, st), "chunk_owner")) err = 1;
+    if (!err) cudaStreamSynchronize(st);  // ws goes out of scope
+  }
   std::vector<double> Xv(X, X + 3 * (size_t)V);
   if (!err && bad(s->d_X.upload(Xv, st), "X")) err = 1;
   if (!err && bad(s->d_io.alloc(3 * (size_t)V), "io")) err = 1;
@@ -847,6 +922,7 @@ int set_params(vbd_solver* s, double dt, double tol, int max_iter) {
   p.g[2] = s->g[2];
   p.max_iter = max_iter;
   p.strict_spd = (s->flags & VBD_STRICT_SPD) ? 1 : 0;
+  p.warm = s->warm ? 1 : 0;
   if (s->params_valid && std::memcmp(&p, &s->cur_params, sizeof p) == 0) return VBD_OK;
   // the pinned staging struct may still be read by an earlier copy
   CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -923,6 +999,13 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
                           cudaMemcpyHostToDevice));
       dtol = s->d_tol.p;
     }
+    if (s->warm) {
+      // features of the coming step, then the network's predicted corrections
+      CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
+                                  s->ws_history ? 1 : 0, s->d_feat.p, st));
+      CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
+                               s->d_pred.p, st));
+    }
     CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
                              s->d_work.p, (int)s->work.size(), s->cluster, s->smem_bytes, st));
   } else if (s->mode == VBD_MODE_GRAPH) {
@@ -948,6 +1031,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
     CUDA_TRY(launch_end(s->state64, m, s->d_params.p, s->d_ctl.p, st));
   }
   s->pending = true;
+  s->ws_history = true;  // ut now holds this step's inertia target
   return VBD_OK;
 }
 
@@ -963,6 +1047,9 @@ int finish(vbd_solver* s, int* iters_out) {
   s->last_status = status_from_bits(s, s->h_status);
   if (s->replan) {
     // re-balance the next step from this step's sweep counts (stream is idle)
+    s->env_sweeps.resize(s->n_env, 1.0);
+    for (int e = 0; e < s->n_env; ++e)
+      s->env_sweeps[e] = std::max((double)s->h_iters[e], 0.9 * s->env_sweeps[e]);
     const int rc = upload_plan(s, s->h_iters);
     if (rc != VBD_OK) return rc;
   }
@@ -1060,6 +1147,7 @@ int vbd_reset(vbd_solver* s) {
   CUDA_TRY(cudaMemsetAsync(s->d_u.p, 0, sb, s->stream));
   CUDA_TRY(cudaMemsetAsync(s->d_vel.p, 0, sb, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
+  s->ws_history = false;
   return VBD_OK;
 }
 
@@ -1112,6 +1200,7 @@ static int exchange(vbd_solver* s, const double* in, double* out, bool positions
   const size_t bytes = sizeof(double) * 3 * (size_t)s->V;
   void* state = positions ? (void*)s->d_u.p : (void*)s->d_vel.p;
   const double* off = positions ? s->d_X.p : nullptr;
+  if (in) s->ws_history = false;  // a new state: no previous inertia target
   if (out) {
     CUDA_TRY(launch_gather(s->state64, off, s->d_map.p, state, s->d_io.p, s->V, st));
     CUDA_TRY(cudaMemcpyAsync(out, s->d_io.p, bytes, cudaMemcpyDeviceToHost, st));
@@ -1162,6 +1251,122 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
 }
 
 void* vbd_get_stream(vbd_solver* s) { return s ? (void*)s->stream : nullptr; }
+
+// ---- learned warm start ----------------------------------------------------
+int vbd_ws_param_count(void) { return kWsParams; }
+int vbd_ws_feature_width(void) { return kWsRow; }
+
+static int ensure_ws_buffers(vbd_solver* s) {
+  if (!s->d_feat.p) {
+    CUDA_TRY(s->d_feat.alloc((size_t)s->V * kWsRow));
+    // rows of vertices that are never solved keep flag 0
+    CUDA_TRY(cudaMemsetAsync(s->d_feat.p, 0, sizeof(float) * (size_t)s->V * kWsRow, s->stream));
+  }
+  if (!s->d_pred.p) CUDA_TRY(s->d_pred.alloc((size_t)s->V));
+  return VBD_OK;
+}
+
+int vbd_set_warmstart(vbd_solver* s, const float* params, const float* norm) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  DeviceGuard dg(s->device);
+  if (!params) {
+    s->warm = false;
+    return VBD_OK;
+  }
+  if (s->mode != VBD_MODE_BLOCK)
+    return fail(VBD_ERR_UNSUPPORTED, "the learned warm start runs in block mode");
+  for (int i = 0; i < kWsParams; ++i)
+    if (!std::isfinite(params[i])) return fail(VBD_ERR_INVALID_ARG, "non-finite parameter");
+  std::vector<float> nrm(kWsNorm);
+  for (int i = 0; i < kWsNorm; ++i) {
+    // identity normalisation: mean 0, 1/std 1, std 1, mean 0
+    const bool scale = (i >= kWsIn && i < 2 * kWsIn) || (i >= 2 * kWsIn && i < 2 * kWsIn + kWsOut);
+    nrm[i] = norm ? norm[i] : (scale ? 1.0f : 0.0f);
+    if (!std::isfinite(nrm[i])) return fail(VBD_ERR_INVALID_ARG, "non-finite normalisation");
+  }
+  int rc = ensure_ws_buffers(s);
+  if (rc != VBD_OK) return rc;
+  if (!s->d_wparams.p) CUDA_TRY(s->d_wparams.alloc(kWsParams));
+  if (!s->d_wbf.p) CUDA_TRY(s->d_wbf.alloc(2 * (size_t)kWsParams));
+  if (!s->d_wnorm.p) CUDA_TRY(s->d_wnorm.alloc(kWsNorm));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  CUDA_TRY(cudaMemcpy(s->d_wnorm.p, nrm.data(), sizeof(float) * kWsNorm, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(s->d_wparams.p, params, sizeof(float) * kWsParams, cudaMemcpyHostToDevice));
+  CUDA_TRY(launch_to_bf16(s->d_wparams.p, s->d_wbf.p, kWsParams, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  s->warm = true;
+  return VBD_OK;
+}
+
+int vbd_ws_features(vbd_solver* s, double dt, float* features) {
+  if (!s || !features) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  if (!(dt > 0.0)) return fail(VBD_ERR_INVALID_ARG, "dt must be > 0");
+  DeviceGuard dg(s->device);
+  int rc = ensure_ws_buffers(s);
+  if (rc != VBD_OK) return rc;
+  CUDA_TRY(cudaMemsetAsync(features, 0, sizeof(float) * (size_t)s->V * kWsRow, s->stream));
+  CUDA_TRY(launch_ws_features(s->prec, s->tpv, s->mesh(), (int)s->L.chunk.size(), dt, s->g,
+                              s->ws_history ? 1 : 0, features, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return VBD_OK;
+}
+
+int vbd_ws_predict(vbd_solver* s, const float* features, float* predictions) {
+  if (!s || !features || !predictions) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  if (!s->d_wbf.p || !s->d_wnorm.p)
+    return fail(VBD_ERR_INVALID_ARG, "no warm-start model set (vbd_set_warmstart)");
+  DeviceGuard dg(s->device);
+  CUDA_TRY(launch_ws_infer(features, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
+                           reinterpret_cast<float4*>(predictions), s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return VBD_OK;
+}
+
+int vbd_get_env_status(vbd_solver* s, uint32_t* status_out) {
+  if (!s || !status_out) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  DeviceGuard dg(s->device);
+  if (s->pending) {
+    const int rc = finish(s, nullptr);
+    if (rc < 0) return rc;
+  }
+  std::memcpy(status_out, s->h_status, sizeof(uint32_t) * s->n_env);
+  return VBD_OK;
+}
+
+int vbd_ws_targets(vbd_solver* s, const float* features, float* targets) {
+  if (!s || !features || !targets) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  DeviceGuard dg(s->device);
+  CUDA_TRY(launch_ws_targets(s->state64, s->mesh(), features, targets, s->stream));
+  CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return VBD_OK;
+}
+
+int vbd_mlp_train_batch(const float* X, const float* Y, const int32_t* idx, int batch,
+                        const float* params, float* grad, float* scratch, double* loss,
+                        void* stream) {
+  if (!X || !Y || !params || !grad || !scratch || batch <= 0)
+    return fail(VBD_ERR_INVALID_ARG, "bad arguments");
+  CUDA_TRY(launch_mlp_train_batch(X, Y, idx, batch, params, grad, scratch, loss,
+                                  static_cast<cudaStream_t>(stream)));
+  return VBD_OK;
+}
+
+int vbd_mlp_forward(const float* X, int n, const float* params, float* out, float* scratch,
+                    void* stream) {
+  if (!X || !params || !out || !scratch || n < 0) return fail(VBD_ERR_INVALID_ARG, "bad arguments");
+  if (n == 0) return VBD_OK;
+  CUDA_TRY(launch_mlp_forward(X, n, params, out, scratch, static_cast<cudaStream_t>(stream)));
+  return VBD_OK;
+}
+
+int vbd_mlp_adam(float* params, const float* grad, float* m, float* v, int n, float lr,
+                 float beta1, float beta2, float eps, int t, void* stream) {
+  if (!params || !grad || !m || !v || n <= 0 || t < 1)
+    return fail(VBD_ERR_INVALID_ARG, "bad arguments");
+  CUDA_TRY(launch_adam(params, grad, m, v, n, lr, beta1, beta2, eps, t,
+                       static_cast<cudaStream_t>(stream)));
+  return VBD_OK;
+}
 
 // Allocation-free step (see vbd_noalloc.cu for who needs it and the limits of
 // its static scratch).  Runs the grid-mode colour sweep one sweep at a time

@@ -34,6 +34,7 @@ enum StatusBits : unsigned {
   kStatGuard = 2u,      // a 3x3 block was not positive definite
   kStatIterCap = 4u,    // max_iter reached without convergence
   kStatTimeout = 8u,
+  kStatWarmUsed = 16u,  // the step started from the learned prediction
 };
 
 struct EnvInfo {
@@ -61,6 +62,8 @@ struct StepParams {
   double g[3];
   int max_iter;
   int strict_spd;
+  int warm;  // start from the learned prediction (DevMesh::ws_pred) when it lowers the energy
+  int pad;
 };
 
 // Grid-mode loop control (one per solver).
@@ -96,6 +99,10 @@ struct DevMesh {
   int n_env;
   int n_vertices;
   int fmt;  // RecordFormat
+  // learned warm start
+  const float4* wstat;      // per vertex: h, log10(E / (rho h^2)), nu, valence / 20
+  const int2* chunk_owner;  // per chunk: (colour index, environment)
+  const float4* ws_pred;    // per vertex: predicted correction (xyz), w = 1 if predicted
 };
 
 }  // namespace vbd

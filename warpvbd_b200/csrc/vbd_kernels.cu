@@ -140,6 +140,80 @@ __device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, co
   }
 }
 
+// Incremental potential of an environment at its block's replica, summed over
+// the group: every block sums its share of the chunks, the block sums are
+// exchanged through distributed shared memory (slot `buf` of s_esum).
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
+__device__ double env_energy(const DevMesh& m, const EnvInfo& e, const SmemState<SReal>& st,
+                             int rank, int g, const StepConst& sc, bool inertia, double* s_sum,
+                             double (*s_esum)[kMaxGroup], int buf) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  double acc = 0.0;
+  for (int c = 0; c < e.ncolors; ++c) {
+    const ColorInfo ci = m.color[e.cbase + c];
+    for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
+      acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, st, sc, inertia);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if (lane == 0) s_sum[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int i = 0; i < nwarps; ++i) v += s_sum[i];
+    s_sum[32] = v;
+  }
+  if (GROUP && g > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    if (threadIdx.x == 0)
+      for (int r = 0; r < g; ++r) *cl.map_shared_rank(&s_esum[buf][rank], r) = s_sum[32];
+    cl.sync();
+    if (threadIdx.x == 0) {
+      double v = 0.0;
+      for (int r = 0; r < g; ++r) v += s_esum[buf][r];
+      s_sum[32] = v;
+    }
+  }
+  __syncthreads();
+  const double v = s_sum[32];
+  __syncthreads();  // s_sum is reused by the next call
+  return v;
+}
+
+// Learned warm start: compare the incremental potential at the inertia guess
+// (the replica's current content) with the one at inertia guess + predicted
+// correction, and keep whichever is lower.  Every block of a group decides
+// the same way from the same sums.  Returns kStatWarmUsed or 0.
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
+__device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
+                                     const SmemState<SReal>& local, int rank, int g,
+                                     const StepConst& sc, double* s_sum,
+                                     double (*s_esum)[kMaxGroup]) {
+  using S4 = real4<SReal>;
+  const double e0 =
+      env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, false, s_sum, s_esum, 0);
+  for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x) {
+    const float4 d = m.ws_pred[e.vbase + i];
+    if (d.w > 0.f) {
+      S4 v = local.load(i);
+      v.x += SReal(d.x);
+      v.y += SReal(d.y);
+      v.z += SReal(d.z);
+      local.store(i, v);
+    }
+  }
+  __syncthreads();
+  const double e1 =
+      env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, true, s_sum, s_esum, 1);
+  const bool accept = e1 < e0;  // false on NaN as well
+  if (!accept) {
+    // back to the inertia guess, exactly as begin computed it
+    for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x)
+      local.store(i, ldcg4(reinterpret_cast<const S4*>(m.ut) + e.vbase + i));
+  }
+  return accept ? (unsigned)kStatWarmUsed : 0u;
+}
+
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
 __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
                                                         const double* __restrict__ tol_env,
@@ -149,6 +223,8 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
   SReal* sp = reinterpret_cast<SReal*>(smem_raw);
   __shared__ unsigned long long s_red[32];
   __shared__ unsigned long long s_conv[2][kMaxGroup];
+  __shared__ double s_sum[33];
+  __shared__ double s_esum[2][kMaxGroup];
   __shared__ int s_done;
   __shared__ unsigned s_stat;
   const int4 w = work[blockIdx.x];
@@ -170,10 +246,20 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     cg::cluster_group cl = cg::this_cluster();
     const GroupSmemState<SReal> su{sp, g, rank};
     cl.sync();  // every block of the group has started and filled its replica
+    if (p.warm && m.ws_pred) {
+      stat |= warm_start_stage<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, s_sum,
+                                                                 s_esum);
+      cl.sync();  // replicas settled before the first remote update
+    }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, su, rank, g, sc, p.max_iter, tol,
                                                         stat, converged, s_red, s_conv, &s_done);
   } else {
     __syncthreads();
+    if (p.warm && m.ws_pred) {
+      stat |= warm_start_stage<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, s_sum,
+                                                                 s_esum);
+      __syncthreads();
+    }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, p.max_iter, tol,
                                                         stat, converged, s_red, s_conv, &s_done);
   }

@@ -55,6 +55,45 @@ def _device_index(device):
                      "there is no CPU path")
 
 
+def _set_warmstart(handle, model):
+    """Enable the learned warm start, or disable it (None).  `model` is a
+    (params, norm) pair as returned by warmstart.load / train_warmstart, or
+    bare parameters (identity normalisation)."""
+    L = _lib.load()
+    if model is None:
+        return _lib.check(L.vbd_set_warmstart(handle, None, None), "vbd_set_warmstart")
+    params, norm = model if isinstance(model, tuple) else (model, None)
+    fp = ctypes.POINTER(ctypes.c_float)
+    p = np.ascontiguousarray(np.asarray(params, np.float32).reshape(-1))
+    if p.size != L.vbd_ws_param_count():
+        raise ValueError(f"expected {L.vbd_ws_param_count()} parameters, got {p.size}")
+    n = None if norm is None else np.ascontiguousarray(np.asarray(norm, np.float32).reshape(-1))
+    if n is not None and n.size != 50:
+        raise ValueError("the normalisation vector holds 50 values")
+    return _lib.check(L.vbd_set_warmstart(handle, p.ctypes.data_as(fp),
+                                          None if n is None else n.ctypes.data_as(fp)),
+                      "vbd_set_warmstart")
+
+
+def _ws_features(handle, n, dt, out):
+    import torch
+    L = _lib.load()
+    if out is None:
+        out = torch.empty((n, L.vbd_ws_feature_width()), device="cuda")
+    _lib.check(L.vbd_ws_features(handle, float(dt), ctypes.c_void_p(out.data_ptr())),
+               "vbd_ws_features")
+    return out
+
+
+def _ws_targets(handle, n, features, out):
+    import torch
+    if out is None:
+        out = torch.empty((n, 3), device=features.device)
+    _lib.check(_lib.load().vbd_ws_targets(handle, ctypes.c_void_p(features.data_ptr()),
+                                          ctypes.c_void_p(out.data_ptr())), "vbd_ws_targets")
+    return out
+
+
 class DeviceArray:
     """A vertex array (positions or velocities) held on the GPU by a solver.
 
@@ -299,6 +338,18 @@ class VBDSolver:
         if iterations == max_iter:   # the reference's warning condition (vbd_solver.py:581-582)
             print("Warning: VBD solver did not converge within the maximum number of "
                   "iterations.")
+
+    # ---- learned warm start (see warpvbd_b200.warmstart) --------------------
+    def set_warmstart(self, params):
+        """Start every step from the network's prediction when it lowers the
+        incremental potential (params: fp32 array, None disables)."""
+        return _set_warmstart(self._h, params)
+
+    def ws_features(self, dt, out=None):
+        return _ws_features(self._h, self.n_vertices, dt, out)
+
+    def ws_targets(self, features, out=None):
+        return _ws_targets(self._h, self.n_vertices, features, out)
 
     def close(self):
         h = getattr(self, "_h", None)
