@@ -118,7 +118,7 @@ def profile_traffic_per_slot(kernel, workload):
     path = os.path.join(ROOT, "profiles", f"{kernel}.{workload}.md")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_slot_visit:"):
+            if line.strip().startswith("dram_bytes_per_slot_visit:"):
                 return float(line.split(":")[1])
     except OSError:
         pass
