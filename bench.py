@@ -40,6 +40,7 @@ from warpvbd_b200 import scenes  # noqa: E402
 DT = 1e-3
 TOL = 1e-7
 MAX_ITER = 1000
+MODE_NAMES = {0x100: "block", 0x200: "graph", 0x300: "hostloop", 0x400: "persist"}
 
 
 def make_workload(name):
@@ -298,18 +299,20 @@ def run_ours(args, envs, desc, batched):
     b_sweep = np.array([p[0] for p in per_env])
     slots = np.array([p[2] for p in per_env])
     solved = np.array([p[1] for p in per_env])
-    mode = {0x100: "block", 0x200: "graph", 0x300: "hostloop"}[info["mode"]]
+    mode = MODE_NAMES[info["mode"]]
     # sweeps, plus the two energy passes over every slot when the warm start
     # compares the prediction with the inertia guess
     passes = iters + (2 if warm is not None else 0)
     alg_bytes = float((passes * b_sweep[None, :]).sum())
     achieved = alg_bytes / (total_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
-    kernel = "env_step_kernel" if mode == "block" else "color_kernel"
+    kernel = {"block": "env_step_kernel", "persist": "persist_kernel"}.get(mode, "color_kernel")
     tps = profile_traffic_per_slot(kernel, args.workload)
     traffic = None if tps is None else tps * float((passes * slots[None, :]).sum()) / args.steps
-    launches = args.steps if mode == "block" else int(
-        args.steps * 2 + iters.sum() * (info["n_colors"] + 1))
+    if mode in ("block", "persist"):
+        launches = args.steps  # one kernel per step (persist: plus a memset of its control word)
+    else:
+        launches = int(args.steps * 2 + iters.sum() * (info["n_colors"] + 1))
     line = {"metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -389,8 +392,7 @@ def run_ours(args, envs, desc, batched):
         line["cantilever160"] = {
             "sim_s_per_wall_s": args.secondary_steps * DT / t,
             "ms_per_step": 1e3 * t / args.secondary_steps,
-            "iters_per_step": float(cit.mean()), "mode": {0x100: "block", 0x200: "graph"}.get(
-                cs.info()["mode"], "hostloop"),
+            "iters_per_step": float(cit.mean()), "mode": MODE_NAMES[cs.info()["mode"]],
             "vertex_updates_per_s": csolved * float(cit.sum()) / t,
             "roofline_frac": cb * float(cit.sum()) / t / 1e9 / peak}
         cs.close()
@@ -408,7 +410,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch256")
-    ap.add_argument("--mode", default="auto", choices=["auto", "block", "graph", "hostloop"])
+    ap.add_argument("--mode", default="auto",
+                    choices=["auto", "block", "graph", "hostloop", "persist"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--secondary-steps", type=int, default=30)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)

@@ -63,6 +63,9 @@ typedef struct vbd_solver vbd_solver;
 #define VBD_MODE_BLOCK 0x100    /* one thread block per environment runs the whole step */
 #define VBD_MODE_GRAPH 0x200    /* per-colour kernels looped by a CUDA-graph conditional node */
 #define VBD_MODE_HOSTLOOP 0x300 /* per-colour kernels, the host reads the convergence test each sweep */
+/* one cooperative launch per step: resident blocks run every colour of every
+ * sweep, separated by bounded grid barriers (one environment) */
+#define VBD_MODE_PERSIST 0x400
 #define VBD_MODE_MASK 0xF00
 #define VBD_ORDER_INDEX 0x1000  /* keep ascending vertex index inside a colour (default: by valence) */
 /* fail a step instead of taking the guarded fallback when a 3x3 block is not
@@ -120,6 +123,13 @@ int vbd_create_batched(const double* rest_positions, int n_vertices, const int32
                        vbd_solver** out);
 
 void vbd_destroy(vbd_solver* s);
+
+/* No counterpart in the reference.  Bounds every device-side wait of the
+ * persistent mode (VBD_MODE_PERSIST grid barriers): a wait gives up after
+ * max_polls polls or max_wait_ns nanoseconds, whichever comes first, and the
+ * step then fails with VBD_ERR_TIMEOUT (positions undefined until
+ * vbd_reset / vbd_set_positions).  Defaults: 2^26 polls, 2 s. */
+int vbd_set_wait_limits(vbd_solver* s, long long max_polls, unsigned long long max_wait_ns);
 
 /* VBDSolver.reset (vbd_solver.py:501-506): positions back to rest, velocity 0 */
 int vbd_reset(vbd_solver* s);

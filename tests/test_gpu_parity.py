@@ -44,12 +44,13 @@ def run_pair(s, steps, material="snh", kd=0.0, precision="mixed", mode="auto", t
     return gpu, orc, xg, xo, np.array(its_g), np.array(its_o), worst
 
 
-@pytest.mark.parametrize("mode", ["block", "graph", "hostloop"])
+@pytest.mark.parametrize("mode", ["block", "graph", "hostloop", "persist"])
 def test_cantilever_20x2x2_300_steps(mode):
     s = scenes.cantilever(20)
     steps = 300 if mode != "hostloop" else 60
     gpu, orc, xg, xo, ig, io, worst = run_pair(s, steps, mode=mode)
-    assert gpu.info()["mode"] == {"block": 0x100, "graph": 0x200, "hostloop": 0x300}[mode]
+    assert gpu.info()["mode"] == {"block": 0x100, "graph": 0x200, "hostloop": 0x300,
+                                  "persist": 0x400}[mode]
     assert worst < POS_TOL, worst
     dg, do = _tip_disp(xg, s), _tip_disp(xo, s)
     rel = np.linalg.norm(dg - do) / np.linalg.norm(do)

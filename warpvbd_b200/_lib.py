@@ -41,7 +41,9 @@ ORDER_INDEX = 0x1000
 STRICT_SPD = 0x2000
 CLUSTER_SHIFT = 16
 
-MODES = {"auto": MODE_AUTO, "block": MODE_BLOCK, "graph": MODE_GRAPH, "hostloop": MODE_HOSTLOOP}
+MODE_PERSIST = 0x400
+MODES = {"auto": MODE_AUTO, "block": MODE_BLOCK, "graph": MODE_GRAPH, "hostloop": MODE_HOSTLOOP,
+         "persist": MODE_PERSIST}
 
 _d = ctypes.POINTER(ctypes.c_double)
 _i = ctypes.POINTER(ctypes.c_int32)
@@ -75,6 +77,7 @@ SIGNATURES = {
                                           ctypes.c_int, ctypes.POINTER(_vp)]),
     "vbd_destroy": (None, [_vp]),
     "vbd_reset": (ctypes.c_int, [_vp]),
+    "vbd_set_wait_limits": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_ulonglong]),
     "vbd_step": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip]),
     "vbd_step_batched": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _d,
                                         ctypes.c_int, _ip]),

@@ -244,6 +244,36 @@ __device__ __forceinline__ int4 load_slot(const DevMesh& m, size_t i) {
   return __ldg(m.rec_idx + i);
 }
 
+// A slot as stored (kept packed in registers while prefetched).
+template <int FMT>
+struct RawSlot;
+template <>
+struct RawSlot<kFmtIdx16> {
+  using type = ushort4;
+  static __device__ __forceinline__ ushort4 load(const DevMesh& m, size_t i) {
+    return __ldg(m.rec_idx16 + i);
+  }
+  static __device__ __forceinline__ int4 unpack(const ushort4& s) {
+    return make_int4(s.x, s.y, s.z, s.w);
+  }
+};
+template <>
+struct RawSlot<kFmtIdx32> {
+  using type = int4;
+  static __device__ __forceinline__ int4 load(const DevMesh& m, size_t i) {
+    return __ldg(m.rec_idx + i);
+  }
+  static __device__ __forceinline__ int4 unpack(const int4& s) { return s; }
+};
+
+// Slot steps of a chunk whose indices are loaded up front: enough for the
+// reference's 20 incident tets per vertex (MAX_ELEMENTS_PER_VERTEX); longer
+// chunks stream the rest.
+template <int TPV>
+struct Prefetch {
+  static constexpr int steps = (20 + TPV - 1) / TPV;
+};
+
 // ---------------------------------------------------------------------------
 // One warp processes one chunk (32/TPV vertices of one colour).  `st` reads
 // and writes the environment's displacements by environment-local id.
@@ -261,35 +291,50 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
   const bool valid = gv < ci.vend;
   const int lv = gv - vbase;
   const ChunkInfo ch = m.chunk[q];
+  // Every load that does not depend on another is issued here, before the
+  // first use: the chunk's slot indices (all steps up to the prefetch
+  // depth; the SELL blocks are padded, so every lane's load is in bounds),
+  // the vertex's valence, position and inertia target.
+  using RS = RawSlot<FMT>;
+  constexpr int PF = Prefetch<TPV>::steps;
+  const size_t base = (size_t)ch.block * 32 + lane;
+  typename RS::type sl[PF];
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps) sl[s] = RS::load(m, base + (size_t)s * 32);
   int k = 0;
-  S4 uo;
+  S4 uo, tt;
   uo.x = uo.y = uo.z = uo.w = SReal(0);
+  tt = uo;
   if (valid) {
     k = __ldg(m.valence + gv);
     uo = st.load(lv);
+    // ut / up are written in this launch by another block of a group: read
+    // them through L2, past a possibly stale L1 line
+    if (sub == 0) tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
   }
   Real g[3] = {Real(0), Real(0), Real(0)};
   Real h[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
   const R4* tab = reinterpret_cast<const R4*>(m.rec_tab);
-  const size_t base = (size_t)ch.block * 32 + lane;
-#pragma unroll 2
-  for (int s = 0; s < ch.steps; ++s) {
-    if (s * TPV + sub < k) {
-      const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
-      const R4* t = tab + 3 * (size_t)id.w;
-      const R4 q0 = ldg4(t);
-      const R4 q1 = ldg4(t + 1);
-      const R4 q2 = ldg4(t + 2);
-      const S4 a = st.load(id.x);
-      const S4 b = st.load(id.y);
-      const S4 c = st.load(id.z);
-      // neighbour offsets formed in the state precision, then rounded
-      slot_accumulate<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
-                                 Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
-                                 Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z), q0, q1,
-                                 q2, g, h);
-    }
-  }
+  auto visit = [&](const int4& id) {
+    const R4* t = tab + 3 * (size_t)id.w;
+    const R4 q0 = ldg4(t);
+    const R4 q1 = ldg4(t + 1);
+    const R4 q2 = ldg4(t + 2);
+    const S4 a = st.load(id.x);
+    const S4 b = st.load(id.y);
+    const S4 c = st.load(id.z);
+    // neighbour offsets formed in the state precision, then rounded
+    slot_accumulate<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                               Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                               Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z), q0, q1, q2,
+                               g, h);
+  };
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps && s * TPV + sub < k) visit(RS::unpack(sl[s]));
+  for (int s = PF; s < ch.steps; ++s)
+    if (s * TPV + sub < k) visit(load_slot<FMT>(m, base + (size_t)s * 32));
 #pragma unroll
   for (int off = TPV / 2; off > 0; off >>= 1) {
 #pragma unroll
@@ -298,9 +343,6 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
     for (int i = 0; i < 6; ++i) h[i] += __shfl_xor_sync(0xffffffffu, h[i], off);
   }
   if (valid && sub == 0) {
-    // ut / up are written in this launch by another block of a group: read
-    // them through L2, past a possibly stale L1 line
-    const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
     const Real mdt2 = Real(tt.w * SReal(sc.inv_dt2));
     Real G[3], H[6];
     G[0] = g[0] + mdt2 * Real(uo.x - tt.x);

@@ -22,6 +22,7 @@
 #include "../../include/vbd_b200.h"
 #include "vbd_internal.h"
 #include "vbd_launch.h"
+#include "vbd_persist.h"
 #include "vbd_noalloc.h"
 #include "vbd_warmstart.h"
 
@@ -455,6 +456,9 @@ struct vbd_solver {
   DevBuf<double> d_X, d_io, d_tol;
   DevBuf<StepParams> d_params;
   DevBuf<LoopControl> d_ctl;
+  DevBuf<PersistCtl> d_pctl;  // persistent mode
+  int persist_blocks = 0;
+  PersistLimits wait_limits{1ll << 26, 2000000000ull};  // every grid-barrier wait
   // block-mode work map: (environment, rank, group size) per thread block
   int cluster = 1;           // blocks per cluster = group size of a split environment
   bool replan = false;       // re-plan from the measured sweep counts after each step
@@ -551,6 +555,7 @@ void free_solver(vbd_solver* s) {
   s->d_wnorm.release();
   s->d_params.release();
   s->d_ctl.release();
+  s->d_pctl.release();
   if (s->h_iters) cudaFreeHost(s->h_iters);
   if (s->h_status) cudaFreeHost(s->h_status);
   if (s->h_params) cudaFreeHost(s->h_params);
@@ -706,9 +711,15 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     delete s;
     return fail(VBD_ERR_UNSUPPORTED, "an environment does not fit in shared memory for block mode");
   }
-  if ((mode == VBD_MODE_GRAPH || mode == VBD_MODE_HOSTLOOP) && s->n_env != 1) {
+  if ((mode == VBD_MODE_GRAPH || mode == VBD_MODE_HOSTLOOP || mode == VBD_MODE_PERSIST) &&
+      s->n_env != 1) {
     delete s;
-    return fail(VBD_ERR_UNSUPPORTED, "graph / host-loop mode runs a single environment");
+    return fail(VBD_ERR_UNSUPPORTED, "graph / host-loop / persistent mode runs a single environment");
+  }
+  if (mode != VBD_MODE_BLOCK && mode != VBD_MODE_GRAPH && mode != VBD_MODE_HOSTLOOP &&
+      mode != VBD_MODE_PERSIST) {
+    delete s;
+    return fail(VBD_ERR_INVALID_ARG, "unknown mode");
   }
   s->mode = mode;
   const bool block_mode = mode == VBD_MODE_BLOCK;
@@ -720,7 +731,7 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   s->cluster = !block_mode ? 1 : (cl ? cl : (s->n_env > 1 ? 4 : 1));
   s->replan = block_mode && s->n_env > 1 && s->cluster > 1;
   if (threads == 0) threads = block_mode ? (s->n_env > 1 ? 256 : 512) : 256;
-  if (!block_mode) threads = 256;
+  if (mode == VBD_MODE_GRAPH || mode == VBD_MODE_HOSTLOOP) threads = 256;
   if (threads % 32 || threads < 32 || threads > 512) {
     delete s;
     return fail(VBD_ERR_INVALID_ARG, "block_threads must be a multiple of 32 in [32, 512]");
@@ -828,6 +839,25 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   if (!err && bad(s->d_status.alloc(s->n_env), "status")) err = 1;
   if (!err && bad(s->d_params.alloc(1), "params")) err = 1;
   if (!err && bad(s->d_ctl.alloc(1), "ctl")) err = 1;
+  if (!err && mode == VBD_MODE_PERSIST) {
+    if (bad(s->d_pctl.alloc(1), "persist ctl")) err = 1;
+    // resident blocks, but no more than the largest colour can keep busy
+    // (one chunk per warp): fewer blocks make cheaper grid barriers
+    int per_sm = 0, sms = 0;
+    if (!err && bad(persist_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads, &per_sm),
+                    "persist occupancy"))
+      err = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int wpb = s->threads / 32;
+    int need = 1;
+    for (const ColorInfo& ci : s->L.color)
+      need = std::max(need, (ci.chunk_end - ci.chunk_begin + wpb - 1) / wpb);
+    s->persist_blocks = std::min(need, per_sm * sms);
+    if (!err && s->persist_blocks < 1) {
+      g_last_error = "persistent mode: the kernel does not fit on the device";
+      err = 1;
+    }
+  }
   const size_t sb = s->real4_bytes * (size_t)V;
   for (auto* b : {&s->d_u, &s->d_ut, &s->d_up, &s->d_vel})
     if (!err && bad(b->alloc(sb), "state")) err = 1;
@@ -1008,6 +1038,9 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
     }
     CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
                              s->d_work.p, (int)s->work.size(), s->cluster, s->smem_bytes, st));
+  } else if (s->mode == VBD_MODE_PERSIST) {
+    CUDA_TRY(launch_persist(s->prec, s->material, s->tpv, s->threads, m, s->d_params.p,
+                            s->d_pctl.p, s->persist_blocks, s->wait_limits, st));
   } else if (s->mode == VBD_MODE_GRAPH) {
     rc = build_graph(s);
     if (rc != VBD_OK) return rc;
@@ -1140,6 +1173,14 @@ int vbd_create_batched(const double* rest_positions, int n_vertices, const int32
 
 void vbd_destroy(vbd_solver* s) { free_solver(s); }
 
+int vbd_set_wait_limits(vbd_solver* s, long long max_polls, unsigned long long max_wait_ns) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  if (max_polls < 0) return fail(VBD_ERR_INVALID_ARG, "max_polls must be >= 0");
+  s->wait_limits.max_polls = max_polls;
+  s->wait_limits.max_wait_ns = max_wait_ns;
+  return VBD_OK;
+}
+
 int vbd_reset(vbd_solver* s) {
   if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
   DeviceGuard dg(s->device);
@@ -1246,7 +1287,7 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
   info->n_unique_records = s->L.table.size();
   info->record_format = s->fmt == kFmtIdx16 ? 8 : 16;
   info->cluster = s->cluster;
-  info->n_blocks = (int)s->work.size();
+  info->n_blocks = s->mode == VBD_MODE_PERSIST ? s->persist_blocks : (int)s->work.size();
   return VBD_OK;
 }
 

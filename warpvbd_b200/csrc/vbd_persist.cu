@@ -1,0 +1,273 @@
+// Persistent mode (one environment): the whole time step -- inertia guess,
+// every colour of every sweep, the convergence test and the velocity update
+// -- in ONE cooperative launch whose blocks stay resident and meet at grid
+// barriers, instead of one kernel (graph node) per colour.
+//
+// The step loop of the reference (vbd_solver.py:509-612: initialise,
+// colour loop with a host sync per launch, abs(dxs.sum(1)).max() < dx_tol
+// after each sweep, velocity update) becomes:
+//
+//   begin     grid-stride over vertices: ut = u + dt v + dt^2 g, up = u,
+//             active vertices start from ut                      | barrier
+//   sweep     for each colour: warps take the colour's chunks grid-stride
+//             and update their vertices (process_chunk); colours are
+//             separated by a grid barrier, except that a run of colours
+//             small enough for one block (<= warps per block chunks) is
+//             done by block 0 alone with __syncthreads between them
+//             end of sweep: block max of |dx_x+dx_y+dx_z| -> atomicMax on
+//             a rotating slot; the grid barrier; every block reads the slot
+//             and takes the same stop decision
+//   end       grid-stride velocity update; block 0 writes sweeps and status
+//
+// Grid barrier: one 64-bit arrival counter, zeroed before every launch;
+// barrier k is passed when the counter reaches k * gridDim.x.  Arrival is a
+// release reduction after __syncthreads + __threadfence, the wait an acquire
+// load.  Every wait is bounded (an iteration cap and a wall-clock limit):
+// on expiry the block sets the abort flag, ORs the timeout bit into the
+// environment's status and returns, and every other block leaves at its
+// next wait, so a launch that is not co-resident ends with VBD_ERR_TIMEOUT
+// instead of hanging.  The environment's status word is zeroed before the
+// launch and only ever OR-ed, so a timeout bit is never overwritten.  The
+// launch is cooperative, which makes co-residency a launch-time check.
+//
+// Memory: vertex positions written in one colour are read by other blocks
+// in later colours.  They are read with plain (weak, L1-cacheable) loads,
+// never the non-coherent read-only path: every such read follows a grid
+// barrier whose acquire (thread 0) and __syncthreads order it after the
+// writing block's release, which the memory model makes visible (the
+// acquire invalidates the SM's L1).
+#include <cuda_runtime.h>
+
+#include "vbd_device.cuh"
+#include "vbd_persist.h"
+
+namespace vbd {
+
+namespace {
+
+// Real4 state in global memory, plain loads (see the note on memory above).
+template <typename SReal>
+struct CoherentState {
+  real4<SReal>* p;
+  __device__ __forceinline__ real4<SReal> load(int i) const { return p[i]; }
+  __device__ __forceinline__ void store(int i, const real4<SReal>& v) const { p[i] = v; }
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p,
+                                                    unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier number target / gridDim.x.  Returns false if the launch is
+// aborting (this block's wait expired, or another block's did).
+__device__ __forceinline__ bool grid_sync(PersistCtl* ctl, unsigned long long target,
+                                          const PersistLimits& lim, int* s_ok) {
+  __syncthreads();
+  if (gridDim.x == 1) return true;  // one block: __syncthreads is the barrier
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    red_release_add_u64(&ctl->arrivals, 1ull);
+    const unsigned long long t0 = globaltimer_ns();
+    for (long long n = 0;; ++n) {
+      if (ld_acquire_u64(&ctl->arrivals) >= target) break;
+      const bool expired = n >= lim.max_polls ||
+                           ((n & 255) == 255 && globaltimer_ns() - t0 > lim.max_wait_ns);
+      if (expired || ld_relaxed_u32(&ctl->abort) != 0u) {
+        if (expired) {
+          atomicOr(&ctl->status, kStatTimeout);
+          atomicExch(&ctl->abort, 1u);
+        }
+        ok = 0;
+        break;
+      }
+      __nanosleep(20);
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+__global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
+                                                      const StepParams* __restrict__ pp,
+                                                      PersistCtl* ctl, PersistLimits lim) {
+  using S4 = real4<SReal>;
+  __shared__ unsigned long long s_red[16];
+  __shared__ int s_ok;
+  const StepConst sc = make_const(*pp);
+  const double tol = pp->tol;
+  const int max_iter = pp->max_iter;
+  const EnvInfo e = m.env[0];
+  const int nb = gridDim.x;
+  const int nwarps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = nb * blockDim.x;
+  S4* U = reinterpret_cast<S4*>(m.u);
+  const CoherentState<SReal> state{U};
+  unsigned long long bar = 0ull;  // arrivals that complete the next barrier
+
+#define VBD_GRID_SYNC()                                       \
+  do {                                                        \
+    bar += nb;                                                \
+    if (!grid_sync(ctl, bar, lim, &s_ok)) {                   \
+      if (threadIdx.x == 0) atomicOr(m.status, kStatTimeout); \
+      return;                                                 \
+    }                                                         \
+  } while (0)
+
+  // begin: inertia target and initial guess
+  for (int i = tid; i < e.nv; i += nthreads)
+    U[e.vbase + i] = begin_vertex<SReal>(m, e.vbase + i, i < e.nact, sc, true);
+  VBD_GRID_SYNC();
+
+  unsigned stat = 0u;
+  int it = 0;
+  bool conv = false, nan = false;
+  for (;;) {
+    unsigned long long cmax = 0ull;
+    for (int c = 0; c < e.ncolors; ++c) {
+      const ColorInfo ci = m.color[e.cbase + c];
+      const int nch = ci.chunk_end - ci.chunk_begin;
+      const bool local = nb > 1 && nch <= nwarps;
+      if (local) {
+        if (blockIdx.x == 0 && warp < nch)
+          process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, ci.chunk_begin + warp, lane,
+                                                    state, sc, cmax, stat);
+      } else {
+        for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
+             q += nb * nwarps)
+          process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, cmax,
+                                                    stat);
+      }
+      if (c + 1 == e.ncolors) break;
+      const ColorInfo cn = m.color[e.cbase + c + 1];
+      const bool next_local = nb > 1 && (cn.chunk_end - cn.chunk_begin) <= nwarps;
+      if (local && next_local) {
+        __syncthreads();  // block 0 did both colours; its writes are block-visible
+      } else {
+        VBD_GRID_SYNC();
+      }
+    }
+    // end of sweep: convergence test over the whole grid
+    cmax = warp_max_u64(cmax);
+    const unsigned wst = __reduce_or_sync(0xffffffffu, stat);
+    if (lane == 0) {
+      s_red[warp] = cmax;
+      if (wst) atomicOr(&ctl->status, wst);
+    }
+    __syncthreads();
+    if (warp == 0) {
+      unsigned long long v = lane < nwarps ? s_red[lane] : 0ull;
+      v = warp_max_u64(v);
+      if (lane == 0 && v) atomicMax(&ctl->conv[it % 3], v);
+    }
+    VBD_GRID_SYNC();
+    const unsigned long long v = ld_relaxed_u64(&ctl->conv[it % 3]);
+    // the slot of two sweeps ago: every block read it before this barrier,
+    // and it is next written after the following one
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->conv[(it + 2) % 3] = 0ull;
+    ++it;
+    nan = v > 0x7ff0000000000000ull;
+    conv = !nan && __longlong_as_double((long long)v) < tol;
+    if (conv || nan || it >= max_iter) break;
+  }
+
+  // end: velocity update
+  for (int i = tid; i < e.nv; i += nthreads) end_vertex<SReal>(m, e.vbase + i, U[e.vbase + i], sc);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned st = ld_relaxed_u32(&ctl->status);
+    if (nan) st |= kStatNonFinite;
+    if (!conv) st |= kStatIterCap;
+    m.iters[0] = it;
+    atomicOr(m.status, st);
+  }
+#undef VBD_GRID_SYNC
+}
+
+cudaLaunchConfig_t persist_config(int blocks, int threads, cudaStream_t s,
+                                  cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+struct PersistLaunch {
+  int blocks, threads;
+  const DevMesh& m;
+  const StepParams* p;
+  PersistCtl* ctl;
+  PersistLimits lim;
+  cudaStream_t s;
+  template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+  cudaError_t run() {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = persist_config(blocks, threads, s, attr);
+    return cudaLaunchKernelEx(&cfg, persist_kernel<Real, SReal, TPV, MAT, FMT>, m, p, ctl, lim);
+  }
+};
+
+struct PersistOccupancy {
+  int threads;
+  int* out;
+  template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+  cudaError_t run() {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        out, persist_kernel<Real, SReal, TPV, MAT, FMT>, threads, 0);
+  }
+};
+
+}  // namespace
+
+cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int threads,
+                              int* blocks_per_sm) {
+  if (threads < 32 || threads > 512 || threads % 32) return cudaErrorInvalidValue;
+  PersistOccupancy f{threads, blocks_per_sm};
+  return dispatch(prec, material, fmt, tpv, f);
+}
+
+cudaError_t launch_persist(int prec, int material, int tpv, int threads, const DevMesh& m,
+                           const StepParams* p, PersistCtl* ctl, int blocks,
+                           const PersistLimits& lim, cudaStream_t s) {
+  if (threads < 32 || threads > 512 || threads % 32 || blocks < 1) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(PersistCtl), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.status, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  PersistLaunch f{blocks, threads, m, p, ctl, lim, s};
+  return dispatch(prec, material, m.fmt, tpv, f);
+}
+
+}  // namespace vbd

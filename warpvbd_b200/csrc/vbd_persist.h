@@ -1,0 +1,38 @@
+// Persistent mode: the whole time step of one environment in one cooperative
+// launch (vbd_persist.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "vbd_internal.h"
+
+namespace vbd {
+
+// Device-side control of one persistent step; zeroed by launch_persist
+// before every launch.
+struct PersistCtl {
+  unsigned long long arrivals;  // grid-barrier arrivals in this step
+  unsigned long long conv[3];   // per-sweep max |dx_x+dx_y+dx_z| bits, slot = sweep % 3
+  unsigned status;              // status bits (kStat*) of every block
+  unsigned abort;               // set when a barrier wait expired
+  unsigned pad[2];
+};
+
+// Bounds of every grid-barrier wait.
+struct PersistLimits {
+  long long max_polls;             // polls of the arrival counter
+  unsigned long long max_wait_ns;  // wall-clock limit
+};
+
+// Resident persist_kernel blocks per SM for `threads` threads.
+cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int threads,
+                              int* blocks_per_sm);
+
+// One time step: clears *ctl and m.status[0], then a cooperative launch of
+// `blocks` blocks (at most the resident count).  Writes m.iters[0] and ORs
+// the step's status bits into m.status[0]; a barrier wait that expired adds
+// kStatTimeout there.
+cudaError_t launch_persist(int prec, int material, int tpv, int threads, const DevMesh& m,
+                           const StepParams* p, PersistCtl* ctl, int blocks,
+                           const PersistLimits& lim, cudaStream_t s);
+
+}  // namespace vbd

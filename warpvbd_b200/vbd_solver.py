@@ -141,7 +141,7 @@ class VBDSolver:
                  "stvk" (St. Venant-Kirchhoff, the reference's commented model)
       precision  "mixed" (default: fp64 positions and velocities, fp32 arithmetic),
                  "fp32" (everything fp32) or "fp64" (everything fp64)
-      mode       "auto", "block", "graph" or "hostloop" (see include/vbd_b200.h)
+      mode       "auto", "block", "graph", "hostloop" or "persist" (see include/vbd_b200.h)
       tpv, block_threads   launch shape (0 = automatic)
       cluster    block mode: spread the mesh over this many thread blocks of one
                  cluster (1, 2, 4, 8, 16; 0 = automatic)
