@@ -201,15 +201,29 @@ def run_reference(args, envs, desc, batched):
     print(json.dumps(line), flush=True)
 
 
-def make_solver(envs, batched, local, mode="auto", warm=None):
+def tuned_config(envs, batched, local, mode="auto", use=True):
+    """The autotuner's cached launch shape for this workload on this GPU
+    (warpvbd_b200/data/autotune_b200.json or the user cache), or None."""
+    if not use or (not batched and mode != "auto"):
+        return None
+    from warpvbd_b200 import autotune
+    dev = f"cuda:{local}"
+    if batched:
+        return autotune.cached_batched(envs, device=dev)
+    return autotune.cached_single(envs[0].solver_kwargs(), device=dev)
+
+
+def make_solver(envs, batched, local, mode="auto", warm=None, tuned=None):
     if batched:
         from warpvbd_b200 import BatchedVBDSolver
-        sol = BatchedVBDSolver(envs, dx_tol=TOL, max_iter=MAX_ITER, device=f"cuda:{local}")
+        sol = BatchedVBDSolver(envs, dx_tol=TOL, max_iter=MAX_ITER, device=f"cuda:{local}",
+                               **(tuned or {}))
     else:
         from warpvbd_b200 import VBDSolver
         s = envs[0]
+        shape = tuned or {"mode": mode}
         sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL,
-                        max_iter=MAX_ITER, device=f"cuda:{local}", mode=mode)
+                        max_iter=MAX_ITER, device=f"cuda:{local}", **shape)
     if warm is not None:
         sol.set_warmstart(warm)
     return sol
@@ -262,7 +276,8 @@ def run_ours(args, envs, desc, batched):
     torch.cuda.set_device(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     warm = warm_params(args, batched)
-    sol = make_solver(envs, batched, local, args.mode, warm)
+    tuned = tuned_config(envs, batched, local, args.mode, not args.no_tune)
+    sol = make_solver(envs, batched, local, args.mode, warm, tuned)
     info = sol.info()
     if world > 1:
         torch.distributed.barrier()
@@ -322,7 +337,9 @@ def run_ours(args, envs, desc, batched):
                        "max_iter": MAX_ITER, "mode": mode, "tpv": info["tpv"],
                        "block_threads": info["block_threads"],
                        "parallelism": f"replicas x{world}",
-                       "warm_start": warm is not None,
+                       "warm_start": warm is not None, "cluster": info["cluster"],
+                       "order_index": bool((tuned or {}).get("order_index", False)),
+                       "autotuned": tuned is not None,
                        "l2": "256 MiB written between timed steps"},
             "iters_per_step": {"mean": float(iters.mean()), "max": int(iters.max()),
                                "min": int(iters.min())},
@@ -352,7 +369,7 @@ def run_ours(args, envs, desc, batched):
         from warpvbd_b200 import warmstart
         sol.close()
         other = None if warm is not None else warmstart.load()
-        ps = make_solver(envs, batched, local, warm=other)
+        ps = make_solver(envs, batched, local, warm=other, tuned=tuned)
         pms, pit, _ = timed_steps(ps, batched, args.steps, args.warmup, local, flush)
         pt = float(pms.sum())
         if world > 1:
@@ -385,7 +402,8 @@ def run_ours(args, envs, desc, batched):
     if rank == 0 and world == 1 and batched and not args.no_secondary:
         # the plain single-mesh solver on the 160x16x16 cantilever
         cant = scenes.cantilever(160)
-        cs = make_solver([cant], False, local)
+        cs = make_solver([cant], False, local,
+                         tuned=tuned_config([cant], False, local, "auto", not args.no_tune))
         cms, cit, _ = timed_steps(cs, False, args.secondary_steps, 3, local, flush)
         cb, csolved, _ = sweep_bytes(cant)
         t = float(cms.sum()) * 1e-3
@@ -418,6 +436,8 @@ def main():
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="ignore the autotuner's cached launch shapes (use the built-in defaults)")
     ap.add_argument("--warmstart", default="off", choices=["off", "on"],
                     help="headline batched run starts steps from the trained network (on); "
                          "the other setting is timed as a secondary figure")

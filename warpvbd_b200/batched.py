@@ -23,9 +23,18 @@ class BatchedVBDSolver:
 
     def __init__(self, envs, damping_coefficient=0.0, gravity=(0.0, 0.0, -9.81), dx_tol=1e-7,
                  max_iter=1000, device="cuda", *, material="snh", precision="mixed",
-                 tpv=0, block_threads=0, cluster=0, order_index=False):
+                 tpv=0, block_threads=0, cluster=0, order_index=False, tune=False):
         """``cluster``: blocks per thread-block cluster (0 = automatic); an
-        environment much heavier than the others runs on a whole cluster."""
+        environment much heavier than the others runs on a whole cluster.
+        ``tune``: pick tpv / block_threads / cluster / order_index with the
+        autotuner (warpvbd_b200.autotune; measured once, then cached)."""
+        if tune:
+            from . import autotune
+            cfg = autotune.tune_batched(envs, material=material, precision=precision,
+                                        device=device, dx_tol=dx_tol, max_iter=max_iter)
+            tpv, block_threads = cfg["tpv"], cfg["block_threads"]
+            cluster, order_index = cfg["cluster"], cfg["order_index"]
+        self.device = device
         Xs, Ts, rho, E, nu, act = [], [], [], [], [], []
         voff, toff = [0], [0]
         for env in envs:

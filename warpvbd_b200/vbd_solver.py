@@ -145,6 +145,10 @@ class VBDSolver:
       tpv, block_threads   launch shape (0 = automatic)
       cluster    block mode: spread the mesh over this many thread blocks of one
                  cluster (1, 2, 4, 8, 16; 0 = automatic)
+      order_index  keep ascending vertex index inside a colour (default: by valence)
+      tune       pick mode / tpv / block_threads / cluster / order_index with the
+                 autotuner (warpvbd_b200.autotune; measured once per mesh and GPU
+                 type, then cached)
       coloring   per-vertex colours to use instead of the greedy colouring
       strict_spd raise instead of taking the guarded step on a non-SPD block
       allow_high_valence  lift the reference's 32 incident-tets limit
@@ -154,8 +158,20 @@ class VBDSolver:
                  damping_coefficient=1.0, active_mask=None, gravity=(0.0, 0.0, -9.81),
                  dx_tol=1e-9, max_iter=100, device="cuda", *, material="snh",
                  precision="mixed", mode="auto", tpv=0, block_threads=0, cluster=0, coloring=None,
-                 strict_spd=False, allow_high_valence=False, verbose=False):
+                 strict_spd=False, allow_high_valence=False, verbose=False, order_index=False,
+                 tune=False):
         L = _lib.load()
+        if tune:
+            from . import autotune
+            cfg = autotune.tune_single(
+                dict(initial_positions=_host(initial_positions), elements=_host(elements),
+                     densities=_host(densities), youngs_modulus=_host(youngs_modulus),
+                     poissons_ratio=_host(poissons_ratio),
+                     active_mask=None if active_mask is None else _host(active_mask)),
+                material=material, precision=precision, device=device,
+                damping_coefficient=damping_coefficient)
+            mode, tpv, block_threads = cfg["mode"], cfg["tpv"], cfg["block_threads"]
+            cluster, order_index = cfg["cluster"], cfg["order_index"]
         X = _lib.f64(_host(initial_positions), (-1, 3))
         tets = _lib.i32(_host(elements)).reshape(-1, 4)
         rho = _lib.f64(_host(densities))
@@ -177,6 +193,8 @@ class VBDSolver:
         flags |= _lib.MODES[mode]
         if strict_spd:
             flags |= _lib.STRICT_SPD
+        if order_index:
+            flags |= _lib.ORDER_INDEX
         flags |= int(cluster) << _lib.CLUSTER_SHIFT
         self.device = device
         self._dev = _device_index(device)
