@@ -201,15 +201,18 @@ def run_reference(args, envs, desc, batched):
     print(json.dumps(line), flush=True)
 
 
-def tuned_config(envs, batched, local, mode="auto", use=True):
+def tuned_config(envs, batched, local, mode="auto", use=True, warm=False):
     """The autotuner's cached launch shape for this workload on this GPU
-    (warpvbd_b200/data/autotune_b200.json or the user cache), or None."""
+    (warpvbd_b200/data/autotune_b200.json or the user cache), or None.
+    `warm`: the shape tuned with the learned warm start on (falls back to
+    the plain shape)."""
     if not use or (not batched and mode != "auto"):
         return None
     from warpvbd_b200 import autotune
     dev = f"cuda:{local}"
     if batched:
-        return autotune.cached_batched(envs, device=dev)
+        return ((autotune.cached_batched(envs, device=dev, warm=True) if warm else None)
+                or autotune.cached_batched(envs, device=dev))
     return autotune.cached_single(envs[0].solver_kwargs(), device=dev)
 
 
@@ -276,7 +279,7 @@ def run_ours(args, envs, desc, batched):
     torch.cuda.set_device(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     warm = warm_params(args, batched)
-    tuned = tuned_config(envs, batched, local, args.mode, not args.no_tune)
+    tuned = tuned_config(envs, batched, local, args.mode, not args.no_tune, warm is not None)
     sol = make_solver(envs, batched, local, args.mode, warm, tuned)
     info = sol.info()
     if world > 1:
@@ -340,6 +343,7 @@ def run_ours(args, envs, desc, batched):
                        "warm_start": warm is not None, "cluster": info["cluster"],
                        "order_index": bool((tuned or {}).get("order_index", False)),
                        "autotuned": tuned is not None,
+                       "tiered": bool((tuned or {}).get("tiered", False)),
                        "l2": "256 MiB written between timed steps"},
             "iters_per_step": {"mean": float(iters.mean()), "max": int(iters.max()),
                                "min": int(iters.min())},
@@ -369,7 +373,9 @@ def run_ours(args, envs, desc, batched):
         from warpvbd_b200 import warmstart
         sol.close()
         other = None if warm is not None else warmstart.load()
-        ps = make_solver(envs, batched, local, warm=other, tuned=tuned)
+        ps = make_solver(envs, batched, local, warm=other,
+                         tuned=tuned_config(envs, batched, local, args.mode, not args.no_tune,
+                                            other is not None))
         pms, pit, _ = timed_steps(ps, batched, args.steps, args.warmup, local, flush)
         pt = float(pms.sum())
         if world > 1:
@@ -380,10 +386,13 @@ def run_ours(args, envs, desc, batched):
         pbytes = float((ppass * b_sweep[None, :]).sum())
         pv = world * n_env * args.steps * DT / (pt * 1e-3)
         key = "warm_start_batched" if other is not None else "plain_batched"
+        pinfo = ps.info()
         line[key] = {
             "value": pv, "ms_per_step": pt / args.steps,
             "iters_per_step": {"mean": float(pit.mean()), "max": int(pit.max())},
-            "roofline_frac": pbytes / (pt * 1e-3) / 1e9 / peak}
+            "roofline_frac": pbytes / (pt * 1e-3) / 1e9 / peak,
+            "shape": {"tpv": pinfo["tpv"], "block_threads": pinfo["block_threads"],
+                      "cluster": pinfo["cluster"]}}
         warm_v, plain_v = (pv, value) if other is not None else (value, pv)
         line["warm_start_speedup_vs_plain_batched"] = warm_v / plain_v
         ps.close()

@@ -71,6 +71,12 @@ typedef struct vbd_solver vbd_solver;
 /* fail a step instead of taking the guarded fallback when a 3x3 block is not
  * positive definite (the reference would produce NaN there) */
 #define VBD_STRICT_SPD 0x2000
+/* batched block mode: the environments the planner splits over a cluster run
+ * in one launch (512 threads per block, shared memory for the largest of
+ * them) and all others, one block each, in a second launch on a second stream
+ * at the same time (block_threads threads, shared memory for the largest of
+ * them, so several blocks share an SM) */
+#define VBD_TIERED 0x4000
 /* block mode: thread blocks per cluster (1, 2, 4, 8, 16; 0 = automatic).  An
  * environment much heavier than the others is split over all blocks of one
  * cluster, which share its state through distributed shared memory. */

@@ -201,3 +201,24 @@ def test_nonconvergence_warning_and_nonfinite(capsys):
     bad[50] = np.nan
     with pytest.raises(FloatingPointError):
         sol.step(bad, 1e-3)
+
+
+@pytest.mark.parametrize("cluster,threads", [(4, 256), (8, 128), (2, 512)])
+def test_tiered_launch_is_bit_identical_to_one_launch(cluster, threads):
+    """Heavy environments on clusters in one launch, the rest one block each
+    in a concurrent second launch: every environment's arithmetic is the
+    same as in the single launch, so positions and sweep counts must agree
+    exactly, step after step (the plan is re-made from the sweep counts after
+    every step, so environments move between the tiers)."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(24, seed=4)
+    one = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, cluster=cluster,
+                           block_threads=threads)
+    two = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, cluster=cluster,
+                           block_threads=threads, tiered=True)
+    for _ in range(12):
+        a = one.step(1e-3)
+        b = two.step(1e-3)
+        assert np.array_equal(a, b)
+    assert np.array_equal(one.positions(), two.positions())
+    assert np.array_equal(one.velocities(), two.velocities())

@@ -117,6 +117,48 @@ def test_rejected_prediction_reproduces_plain_vbd_exactly():
     assert np.array_equal(plain.positions(), warm.positions())
 
 
+def _bf16(a):
+    """Round float32 values to bfloat16 (nearest even), returned as float64."""
+    u = np.asarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def test_tensor_core_inference_matches_fp64_forward():
+    """The tcgen05 inference kernel (bf16 weights and activations, fp32
+    accumulation in TMEM) against the FP64 numpy forward of the same network
+    with the weights rounded to bf16.  The vertex length scale h that the
+    kernel multiplies in is recovered from feature 18 = log10(E dt^2 /
+    (rho h^2)) (every environment here has one material)."""
+    envs = scenes.env_batch(3, seed=21)
+    plain, _ = _pair(envs)
+    params, norm = _trained()
+    plain.set_warmstart((params, norm))
+    for _ in range(3):
+        plain.step(1e-3)
+    dt = 1e-3
+    feat = plain.ws_features(dt)
+    pred = plain.ws_predict(feat).cpu().numpy()
+    f = feat.cpu().numpy().astype(np.float64)
+    solved = f[:, 23] > 0
+    assert np.all(pred[~solved] == 0.0) and np.all(pred[solved, 3] == 1.0)
+    E = np.concatenate([np.full(e.n_vertices, float(e.youngs[0])) for e in envs])
+    rho = np.concatenate([np.full(e.n_vertices, float(e.density[0])) for e in envs])
+    h = np.sqrt(E * dt * dt / (rho * 10.0 ** f[:, 18]))
+    mu, istd = norm[:22].astype(np.float64), norm[22:44].astype(np.float64)
+    sy, my = norm[44:47].astype(np.float64), norm[47:50].astype(np.float64)
+    x = (f[solved, :22] - mu) * istd
+    out, _ = mo.forward(_bf16(params), x)
+    expect = (out * sy + my) * (h[solved] * f[solved, 22])[:, None]
+    got = pred[solved, :3]
+    scale = np.abs(expect).max()
+    err = np.abs(got - expect).max() / scale
+    corr = np.corrcoef(got.ravel(), expect.ravel())[0, 1]
+    print(f"tensor-core inference vs fp64: max error {err:.2e} of the largest output, "
+          f"correlation {corr:.6f}, {solved.sum()} vertices")
+    assert err < 3e-2 and corr > 0.999
+
+
 def _trained():
     if not os.path.exists(ws.DEFAULT_WEIGHTS):
         pytest.fail(f"trained warm-start weights missing: {ws.DEFAULT_WEIGHTS}")

@@ -39,6 +39,7 @@ MODE_GRAPH = 0x200
 MODE_HOSTLOOP = 0x300
 ORDER_INDEX = 0x1000
 STRICT_SPD = 0x2000
+TIERED = 0x4000
 CLUSTER_SHIFT = 16
 
 MODE_PERSIST = 0x400

@@ -55,8 +55,8 @@ SINGLE_SPACE = {
     "graph": {"tpv": [4, 2, 8, 16], "order_index": [False, True]},
 }
 BATCH_SPACE = {
-    "block": {"tpv": [4, 2, 8], "block_threads": [256, 128, 512], "cluster": [4, 1, 2, 8],
-              "order_index": [False, True]},
+    "block": {"tiered": [True, False], "cluster": [4, 8, 2, 16], "tpv": [4, 2, 8],
+              "block_threads": [256, 128, 512], "order_index": [False, True]},
 }
 # Shared memory a block-mode step may use (bytes), and per vertex.
 BLOCK_SMEM_LIMIT = 227 * 1024 - 2048
@@ -252,11 +252,17 @@ def tune_single(solver_kwargs, *, material="snh", precision="mixed", device="cud
 
 
 def tune_batched(envs, *, material="snh", precision="mixed", device="cuda", dt=1e-3,
-                 dx_tol=1e-7, max_iter=1000, steps=4, warmup=2, spaces=None, cache_path=None,
-                 refresh=False, verbose=False):
+                 dx_tol=1e-7, max_iter=1000, steps=12, warmup=4, spaces=None, cache_path=None,
+                 refresh=False, verbose=False, warm=None):
     """Fastest launch shape for a batch of environments: a dict of
     BatchedVBDSolver keyword arguments (tpv, block_threads, cluster,
-    order_index)."""
+    order_index).  Each candidate runs `warmup` + `steps` steps from rest: the
+    sweep counts of a batch grow over its first steps as the motion develops,
+    so a window that is too short favours the wrong shape.
+    With `warm` (a warm-start model, see warpvbd_b200.warmstart)
+    the candidates are timed with the learned warm start on, and the result
+    is cached under its own key: the warm-started sweep counts are far more
+    uneven across environments, which favours other shapes."""
     from .batched import BatchedVBDSolver
 
     def get(env, key, attr):
@@ -268,7 +274,8 @@ def tune_batched(envs, *, material="snh", precision="mixed", device="cuda", dt=1
     verts = np.concatenate([x.reshape(-1) for x in Xs])
     offs = np.cumsum([0] + [x.shape[0] for x in Xs]).astype(np.int64)
     name = _device_name(device)
-    key = mesh_key("batched", tets, verts, offs, material, precision, name)
+    key = mesh_key("batched-warm" if warm is not None else "batched", tets, verts, offs,
+                   material, precision, name)
     if not refresh:
         hit = lookup(key, cache_path)
         if hit is not None:
@@ -276,10 +283,13 @@ def tune_batched(envs, *, material="snh", precision="mixed", device="cuda", dt=1
     spaces = spaces or BATCH_SPACE
 
     def evaluate(cfg):
-        args = {k: cfg[k] for k in ("tpv", "block_threads", "cluster", "order_index") if k in cfg}
+        args = {k: cfg[k] for k in ("tpv", "block_threads", "cluster", "order_index", "tiered")
+                if k in cfg}
         try:
             sol = BatchedVBDSolver(envs, dx_tol=dx_tol, max_iter=max_iter, device=device,
                                    material=material, precision=precision, **args)
+            if warm is not None:
+                sol.set_warmstart(warm)
         except Exception as e:
             if verbose:
                 print("skip", cfg, str(e)[:80])
@@ -295,6 +305,7 @@ def tune_batched(envs, *, material="snh", precision="mixed", device="cuda", dt=1
     t0 = time.perf_counter()
     best, cost, log = search_families(spaces, evaluate)
     cfg = {k: v for k, v in _kwargs(best).items() if k != "mode"}
+    cfg["tiered"] = bool(best.get("tiered", False))
     store(key, cfg, {"ms_per_step": cost, "device": name, "evaluated": len(log),
                      "tune_s": round(time.perf_counter() - t0, 1), "n_env": len(envs),
                      "n_vertices": int(offs[-1])}, cache_path)
@@ -320,14 +331,16 @@ def cached_single(solver_kwargs, *, material="snh", precision="mixed", device="c
                   cache_path)
 
 
-def cached_batched(envs, *, material="snh", precision="mixed", device="cuda", cache_path=None):
-    """The cached configuration of a batch, or None: nothing is measured."""
+def cached_batched(envs, *, material="snh", precision="mixed", device="cuda", cache_path=None,
+                   warm=False):
+    """The cached configuration of a batch (`warm`: tuned with the learned
+    warm start on), or None: nothing is measured."""
     Xs = [np.asarray(e.vertices, np.float64).reshape(-1, 3) for e in envs]
     tets = np.concatenate([np.asarray(e.tets, np.int32).reshape(-1) for e in envs])
     verts = np.concatenate([x.reshape(-1) for x in Xs])
     offs = np.cumsum([0] + [x.shape[0] for x in Xs]).astype(np.int64)
-    return lookup(mesh_key("batched", tets, verts, offs, material, precision,
-                           _device_name(device)), cache_path)
+    return lookup(mesh_key("batched-warm" if warm else "batched", tets, verts, offs, material,
+                           precision, _device_name(device)), cache_path)
 
 
 def benchmark_workload(name):
@@ -353,6 +366,8 @@ def main(argv=None):
     ap.add_argument("--out", default=None, help="cache file (default: the user cache)")
     ap.add_argument("--precision", default="mixed")
     ap.add_argument("--refresh", action="store_true")
+    ap.add_argument("--warm", action="store_true",
+                    help="batched workloads: tune with the committed warm-start model on")
     ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args(argv)
     out = {}
@@ -360,8 +375,12 @@ def main(argv=None):
         envs, batched = benchmark_workload(w)
         t0 = time.perf_counter()
         if batched:
+            warm = None
+            if a.warm:
+                from . import warmstart
+                warm = warmstart.load()
             cfg = tune_batched(envs, precision=a.precision, cache_path=a.out, refresh=a.refresh,
-                               verbose=a.verbose)
+                               verbose=a.verbose, warm=warm)
         else:
             cfg = tune_single(envs[0].solver_kwargs(), precision=a.precision, cache_path=a.out,
                               refresh=a.refresh, verbose=a.verbose)

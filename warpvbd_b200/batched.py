@@ -23,17 +23,23 @@ class BatchedVBDSolver:
 
     def __init__(self, envs, damping_coefficient=0.0, gravity=(0.0, 0.0, -9.81), dx_tol=1e-7,
                  max_iter=1000, device="cuda", *, material="snh", precision="mixed",
-                 tpv=0, block_threads=0, cluster=0, order_index=False, tune=False):
+                 tpv=0, block_threads=0, cluster=0, order_index=False, tiered=False,
+                 tune=False):
         """``cluster``: blocks per thread-block cluster (0 = automatic); an
         environment much heavier than the others runs on a whole cluster.
-        ``tune``: pick tpv / block_threads / cluster / order_index with the
-        autotuner (warpvbd_b200.autotune; measured once, then cached)."""
+        ``tiered``: run the environments split over a cluster in one launch
+        and all others, one block each with shared memory sized for the
+        largest of them, in a second launch beside it.
+        ``tune``: pick tpv / block_threads / cluster / order_index / tiered
+        with the autotuner (warpvbd_b200.autotune; measured once, then
+        cached)."""
         if tune:
             from . import autotune
             cfg = autotune.tune_batched(envs, material=material, precision=precision,
                                         device=device, dx_tol=dx_tol, max_iter=max_iter)
             tpv, block_threads = cfg["tpv"], cfg["block_threads"]
             cluster, order_index = cfg["cluster"], cfg["order_index"]
+            tiered = cfg.get("tiered", False)
         self.device = device
         Xs, Ts, rho, E, nu, act = [], [], [], [], [], []
         voff, toff = [0], [0]
@@ -64,6 +70,8 @@ class BatchedVBDSolver:
         flags |= int(cluster) << _lib.CLUSTER_SHIFT
         if order_index:
             flags |= _lib.ORDER_INDEX
+        if tiered:
+            flags |= _lib.TIERED
         L = _lib.load()
         h = ctypes.c_void_p()
         _lib.check(L.vbd_create_batched(

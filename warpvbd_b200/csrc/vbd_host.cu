@@ -470,6 +470,16 @@ struct vbd_solver {
   std::vector<double> env_sweeps;
   std::vector<int4> work;
   DevBuf<int4> d_work;
+  // tiered block mode (VBD_TIERED): `work` lists the split environments
+  // (heavy launch), `work2` the others, one block each (light launch)
+  bool tiered = false;
+  int heavy_threads = 512;
+  size_t smem_per_vertex = 24;
+  size_t smem_heavy = 0, smem_light = 0;
+  std::vector<int4> work2;
+  DevBuf<int4> d_work2;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // learned warm start
   DevBuf<float4> d_wstat;
   DevBuf<int2> d_chunk_owner;
@@ -478,6 +488,8 @@ struct vbd_solver {
   DevBuf<unsigned char> d_wbf;    // bf16 network parameters
   DevBuf<float> d_wparams;        // fp32 staging for the conversion
   DevBuf<float> d_wnorm;          // input / target normalisation (50 floats)
+  DevBuf<unsigned> d_ws_err;      // set by the tensor-core inference when a wait ran out
+  unsigned* h_ws_err = nullptr;   // pinned copy, read back with every warm step
   bool warm = false;
   bool ws_history = false;        // the previous step's inertia target is in ut
   // pinned host
@@ -546,6 +558,13 @@ void free_solver(vbd_solver* s) {
   s->d_io.release();
   s->d_tol.release();
   s->d_work.release();
+  s->d_work2.release();
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->aux) {
+    cudaStreamSynchronize(s->aux);
+    cudaStreamDestroy(s->aux);
+  }
   s->d_wstat.release();
   s->d_chunk_owner.release();
   s->d_feat.release();
@@ -553,6 +572,7 @@ void free_solver(vbd_solver* s) {
   s->d_wbf.release();
   s->d_wparams.release();
   s->d_wnorm.release();
+  s->d_ws_err.release();
   s->d_params.release();
   s->d_ctl.release();
   s->d_pctl.release();
@@ -560,6 +580,7 @@ void free_solver(vbd_solver* s) {
   if (s->h_status) cudaFreeHost(s->h_status);
   if (s->h_params) cudaFreeHost(s->h_params);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->h_ws_err) cudaFreeHost(s->h_ws_err);
   if (s->stream) cudaStreamDestroy(s->stream);
   cudaSetDevice(prev);
   delete s;
@@ -585,8 +606,10 @@ struct DeviceGuard {
 // The split set is the one with the smallest predicted step time: the
 // largest of (heaviest single-block environment, heaviest split environment
 // / (cluster * efficiency), total work / resident blocks).
-void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work) {
+void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
+               std::vector<int4>& work2) {
   const int n = s->n_env, C = s->cluster;
+  work2.clear();
   std::vector<double> w(n);
   for (int e = 0; e < n; ++e) {
     const double sw = (size_t)e < s->env_sweeps.size() ? s->env_sweeps[e] : 1.0;
@@ -605,8 +628,10 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work) {
     return;
   }
   // parallel efficiency of a split environment (cluster barriers and the
-  // replica broadcasts cost a share of the gain)
-  const double eff = C == 2 ? 0.85 : (C == 4 ? 0.75 : (C == 8 ? 0.6 : 0.45));
+  // replica broadcasts cost a share of the gain); measured on B200 for a
+  // 68K-slot environment at 512 threads: 129 / 77 / 49 / 36 / 36 us per sweep
+  // on 1 / 2 / 4 / 8 / 16 blocks
+  const double eff = C == 2 ? 0.84 : (C == 4 ? 0.66 : (C == 8 ? 0.45 : 0.22));
   const double cap = std::max(1, s->capacity_blocks);
   double total = 0.0;
   for (double x : w) total += x;
@@ -628,6 +653,11 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work) {
   }
   for (int i = 0; i < best_h; ++i)
     for (int r = 0; r < C; ++r) work.push_back(make_int4(order[i], r, C, 0));
+  if (s->tiered) {
+    // the others run one block each in the light launch
+    for (int i = best_h; i < n; ++i) work2.push_back(make_int4(order[i], 0, 1, 0));
+    return;
+  }
   int in_cluster = 0;
   for (int i = best_h; i < n; ++i) {
     work.push_back(make_int4(order[i], 0, 1, 0));
@@ -639,16 +669,34 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work) {
   }
 }
 
+size_t tier_smem(const vbd_solver* s, const std::vector<int4>& w) {
+  int nv = 0;
+  for (const int4& x : w)
+    if (x.x >= 0) nv = std::max(nv, s->L.env[x.x].nv);
+  return (size_t)nv * s->smem_per_vertex;
+}
+
 int upload_plan(vbd_solver* s, const int* iters) {
-  std::vector<int4> w;
-  make_plan(s, iters, w);
-  if (w.size() == s->work.size() &&
-      std::memcmp(w.data(), s->work.data(), w.size() * sizeof(int4)) == 0)
-    return VBD_OK;
-  if (w.size() > s->d_work.n) return fail(VBD_ERR_CUDA, "work map larger than its buffer");
-  // the stream is idle here (create, or after a synchronising step)
-  CUDA_TRY(cudaMemcpy(s->d_work.p, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  std::vector<int4> w, w2;
+  make_plan(s, iters, w, w2);
+  const bool same = w.size() == s->work.size() && w2.size() == s->work2.size() &&
+                    std::memcmp(w.data(), s->work.data(), w.size() * sizeof(int4)) == 0 &&
+                    std::memcmp(w2.data(), s->work2.data(), w2.size() * sizeof(int4)) == 0;
+  if (same) return VBD_OK;
+  if (w.size() > s->d_work.n || w2.size() > s->d_work2.n)
+    return fail(VBD_ERR_CUDA, "work map larger than its buffer");
+  // the streams are idle here (create, or after a synchronising step)
+  if (!w.empty())
+    CUDA_TRY(cudaMemcpy(s->d_work.p, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  if (!w2.empty())
+    CUDA_TRY(
+        cudaMemcpy(s->d_work2.p, w2.data(), w2.size() * sizeof(int4), cudaMemcpyHostToDevice));
   s->work.swap(w);
+  s->work2.swap(w2);
+  if (s->tiered) {
+    s->smem_heavy = tier_smem(s, s->work);
+    s->smem_light = tier_smem(s, s->work2);
+  }
   return VBD_OK;
 }
 
@@ -730,6 +778,7 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   }
   s->cluster = !block_mode ? 1 : (cl ? cl : (s->n_env > 1 ? 4 : 1));
   s->replan = block_mode && s->n_env > 1 && s->cluster > 1;
+  s->tiered = s->replan && (flags & VBD_TIERED) != 0;
   if (threads == 0) threads = block_mode ? (s->n_env > 1 ? 256 : 512) : 256;
   if (mode == VBD_MODE_GRAPH || mode == VBD_MODE_HOSTLOOP) threads = 256;
   if (threads % 32 || threads < 32 || threads > 512) {
@@ -767,6 +816,7 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     return rc;
   }
   s->smem_bytes = (size_t)s->L.max_env_vertices * smem_per_vertex;
+  s->smem_per_vertex = smem_per_vertex;
   s->n_records = (long long)s->L.rec_idx.size();
   // 16-bit slots when every environment-local id and record id fits
   s->fmt = (s->L.max_env_vertices <= 65536 && s->L.table.size() <= 65536) ? kFmtIdx16
@@ -901,13 +951,28 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     s->env_work.assign(s->n_env, 0.0);
     for (int e = 0; e < s->n_env; ++e) s->env_work[e] = 4.0 * (toff[e + 1] - toff[e]) + 1.0;
     int occ = 0;
-    if (bad(env_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads, s->smem_bytes,
-                          s->cluster, &occ),
-            "occupancy"))
-      err = 1;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    s->capacity_blocks = s->cluster > 1 ? occ * s->cluster : occ * sms;
+    if (s->tiered) {
+      // capacity of the light launch (one block per environment) at the
+      // largest environment's shared memory: a lower bound
+      if (bad(env_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads, s->smem_bytes, 1,
+                            &occ),
+              "occupancy"))
+        err = 1;
+      s->capacity_blocks = occ * sms;
+      if (!err && (bad(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking), "stream") ||
+                   bad(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming), "event") ||
+                   bad(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "event")))
+        err = 1;
+      if (!err && bad(s->d_work2.alloc((size_t)s->n_env), "work")) err = 1;
+    } else {
+      if (bad(env_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads, s->smem_bytes,
+                            s->cluster, &occ),
+              "occupancy"))
+        err = 1;
+      s->capacity_blocks = s->cluster > 1 ? occ * s->cluster : occ * sms;
+    }
     if (!err && s->capacity_blocks < 1) {
       g_last_error = "block mode: this launch shape does not fit on the device";
       err = 1;
@@ -1034,10 +1099,32 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
       CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
                                   s->ws_history ? 1 : 0, s->d_feat.p, st));
       CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
-                               s->d_pred.p, st));
+                               s->d_pred.p, s->d_ws_err.p, st));
     }
-    CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
-                             s->d_work.p, (int)s->work.size(), s->cluster, s->smem_bytes, st));
+    if (!s->tiered) {
+      CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
+                               s->d_work.p, (int)s->work.size(), s->cluster, s->smem_bytes, st));
+    } else {
+      // heavy launch first (its clusters need whole groups of free SMs), the
+      // light launch beside it on the second stream, joined before the end
+      const bool two = !s->work.empty() && !s->work2.empty();
+      if (two) CUDA_TRY(cudaEventRecord(s->ev_fork, st));
+      if (!s->work.empty())
+        CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->heavy_threads, m,
+                                 s->cur_params, dtol, s->d_work.p, (int)s->work.size(),
+                                 s->cluster, s->smem_heavy, st));
+      if (!s->work2.empty()) {
+        cudaStream_t ls = two ? s->aux : st;
+        if (two) CUDA_TRY(cudaStreamWaitEvent(ls, s->ev_fork, 0));
+        CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params,
+                                 dtol, s->d_work2.p, (int)s->work2.size(), 1, s->smem_light,
+                                 ls));
+        if (two) {
+          CUDA_TRY(cudaEventRecord(s->ev_join, ls));
+          CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
+        }
+      }
+    }
   } else if (s->mode == VBD_MODE_PERSIST) {
     CUDA_TRY(launch_persist(s->prec, s->material, s->tpv, s->threads, m, s->d_params.p,
                             s->d_pctl.p, s->persist_blocks, s->wait_limits, st));
@@ -1068,16 +1155,34 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
   return VBD_OK;
 }
 
+// The tensor-core inference records a wait that ran out in d_ws_err; the
+// rows it did not finish kept no prediction, so the step itself fell back to
+// the inertia guess, but the caller is told.
+// (*h_ws_err holds the device word once the stream has been synchronised.)
+int ws_error_status(vbd_solver* s) {
+  if (!s->warm || !s->h_ws_err || *s->h_ws_err == 0) return VBD_OK;
+  *s->h_ws_err = 0;
+  CUDA_TRY(cudaMemset(s->d_ws_err.p, 0, sizeof(unsigned)));
+  return fail(VBD_ERR_TIMEOUT, "warm-start inference: a tensor-core wait timed out");
+}
+
 int finish(vbd_solver* s, int* iters_out) {
   cudaStream_t st = s->stream;
   CUDA_TRY(cudaMemcpyAsync(s->h_iters, s->d_iters.p, sizeof(int) * s->n_env,
                            cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaMemcpyAsync(s->h_status, s->d_status.p, sizeof(unsigned) * s->n_env,
                            cudaMemcpyDeviceToHost, st));
+  if (s->warm && s->h_ws_err)
+    CUDA_TRY(cudaMemcpyAsync(s->h_ws_err, s->d_ws_err.p, sizeof(unsigned),
+                             cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   s->pending = false;
   if (iters_out) std::memcpy(iters_out, s->h_iters, sizeof(int) * s->n_env);
   s->last_status = status_from_bits(s, s->h_status);
+  if (s->last_status >= 0) {
+    const int ws = ws_error_status(s);
+    if (ws != VBD_OK) s->last_status = ws;
+  }
   if (s->replan) {
     // re-balance the next step from this step's sweep counts (stream is idle)
     s->env_sweeps.resize(s->n_env, 1.0);
@@ -1287,7 +1392,8 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
   info->n_unique_records = s->L.table.size();
   info->record_format = s->fmt == kFmtIdx16 ? 8 : 16;
   info->cluster = s->cluster;
-  info->n_blocks = s->mode == VBD_MODE_PERSIST ? s->persist_blocks : (int)s->work.size();
+  info->n_blocks = s->mode == VBD_MODE_PERSIST ? s->persist_blocks
+                                                : (int)(s->work.size() + s->work2.size());
   return VBD_OK;
 }
 
@@ -1330,7 +1436,11 @@ int vbd_set_warmstart(vbd_solver* s, const float* params, const float* norm) {
   if (!s->d_wparams.p) CUDA_TRY(s->d_wparams.alloc(kWsParams));
   if (!s->d_wbf.p) CUDA_TRY(s->d_wbf.alloc(2 * (size_t)kWsParams));
   if (!s->d_wnorm.p) CUDA_TRY(s->d_wnorm.alloc(kWsNorm));
+  if (!s->d_ws_err.p) CUDA_TRY(s->d_ws_err.alloc(1));
+  if (!s->h_ws_err) CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&s->h_ws_err), sizeof(unsigned)));
+  *s->h_ws_err = 0;
   CUDA_TRY(cudaStreamSynchronize(s->stream));
+  CUDA_TRY(cudaMemset(s->d_ws_err.p, 0, sizeof(unsigned)));
   CUDA_TRY(cudaMemcpy(s->d_wnorm.p, nrm.data(), sizeof(float) * kWsNorm, cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(s->d_wparams.p, params, sizeof(float) * kWsParams, cudaMemcpyHostToDevice));
   CUDA_TRY(launch_to_bf16(s->d_wparams.p, s->d_wbf.p, kWsParams, s->stream));
@@ -1358,9 +1468,11 @@ int vbd_ws_predict(vbd_solver* s, const float* features, float* predictions) {
     return fail(VBD_ERR_INVALID_ARG, "no warm-start model set (vbd_set_warmstart)");
   DeviceGuard dg(s->device);
   CUDA_TRY(launch_ws_infer(features, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
-                           reinterpret_cast<float4*>(predictions), s->stream));
+                           reinterpret_cast<float4*>(predictions), s->d_ws_err.p, s->stream));
+  CUDA_TRY(cudaMemcpyAsync(s->h_ws_err, s->d_ws_err.p, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
-  return VBD_OK;
+  return ws_error_status(s);
 }
 
 int vbd_get_env_status(vbd_solver* s, uint32_t* status_out) {

@@ -181,37 +181,44 @@ __device__ double env_energy(const DevMesh& m, const EnvInfo& e, const SmemState
 }
 
 // Learned warm start: compare the incremental potential at the inertia guess
-// (the replica's current content) with the one at inertia guess + predicted
-// correction, and keep whichever is lower.  Every block of a group decides
-// the same way from the same sums.  Returns kStatWarmUsed or 0.
+// (the replica's current content) with the one at inertia guess + alpha x
+// predicted correction for alpha = 1, 1/2, 1/4 (a backtracking line search
+// along the prediction: the next alpha is tried only when the previous one
+// did not lower the potential), and keep the first that is lower, else the
+// inertia guess.  Every block of a group decides the same way from the same
+// sums.  Returns kStatWarmUsed or 0.
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
 __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
                                      const SmemState<SReal>& local, int rank, int g,
                                      const StepConst& sc, double* s_sum,
                                      double (*s_esum)[kMaxGroup]) {
   using S4 = real4<SReal>;
+  const S4* UT = reinterpret_cast<const S4*>(m.ut) + e.vbase;
   const double e0 =
       env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, false, s_sum, s_esum, 0);
-  for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x) {
-    const float4 d = m.ws_pred[e.vbase + i];
-    if (d.w > 0.f) {
-      S4 v = local.load(i);
-      v.x += SReal(d.x);
-      v.y += SReal(d.y);
-      v.z += SReal(d.z);
-      local.store(i, v);
+  int buf = 1;
+  for (int trial = 0; trial < 3; ++trial) {
+    // candidate: inertia guess + alpha x prediction, formed from ut each time
+    const SReal alpha = SReal(1.0 / double(1 << trial));
+    for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x) {
+      const float4 d = m.ws_pred[e.vbase + i];
+      if (d.w > 0.f) {
+        S4 v = ldcg4(UT + i);
+        v.x += alpha * SReal(d.x);
+        v.y += alpha * SReal(d.y);
+        v.z += alpha * SReal(d.z);
+        local.store(i, v);
+      }
     }
+    __syncthreads();
+    const double e1 = env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, true,
+                                                                     s_sum, s_esum, buf);
+    buf ^= 1;
+    if (e1 < e0) return (unsigned)kStatWarmUsed;  // false on NaN as well
   }
-  __syncthreads();
-  const double e1 =
-      env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, true, s_sum, s_esum, 1);
-  const bool accept = e1 < e0;  // false on NaN as well
-  if (!accept) {
-    // back to the inertia guess, exactly as begin computed it
-    for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x)
-      local.store(i, ldcg4(reinterpret_cast<const S4*>(m.ut) + e.vbase + i));
-  }
-  return accept ? (unsigned)kStatWarmUsed : 0u;
+  // back to the inertia guess, exactly as begin computed it
+  for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x) local.store(i, ldcg4(UT + i));
+  return 0u;
 }
 
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>

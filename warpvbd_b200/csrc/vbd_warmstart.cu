@@ -9,9 +9,9 @@
 // relatively, on small ones.  Parameters (fp32, this order):
 //   W1[64][22] b1[64] W2[64][64] b2[64] W3[3][64] b3[3]
 // The network acts on normalised inputs and predicts normalised targets;
-// inference applies the fp32 normalisation (mean and 1/std of every input,
-// std and mean of every target) around bf16 weights with fp32 accumulation.
-// Training is fp32.
+// inference (vbd_ws_tc.cu, tensor cores) applies the fp32 normalisation (mean
+// and 1/std of every input, std and mean of every target) around bf16
+// weights and activations with fp32 accumulation.  Training is fp32.
 //
 // Displacement-type features, divided by h and then by s = RMS of the 18:
 //   0-2   inertia displacement of the coming step, v dt + g dt^2
@@ -145,65 +145,6 @@ __global__ void ws_targets_kernel(DevMesh m, const float* __restrict__ feat,
   target[3 * (size_t)i] = solved ? float(double(u.x - t.x) * ih) : 0.0f;
   target[3 * (size_t)i + 1] = solved ? float(double(u.y - t.y) * ih) : 0.0f;
   target[3 * (size_t)i + 2] = solved ? float(double(u.z - t.z) * ih) : 0.0f;
-}
-
-// ---------------------------------------------------------------------------
-// Inference: one thread per vertex, bf16 weights in shared memory (the whole
-// network, 11.5 KB), fp32 activations in registers; layers 2 and 3 are fused
-// so the second hidden layer never needs storing.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) ws_infer_kernel(const float* __restrict__ feat, int n,
-                                                       const __nv_bfloat16* __restrict__ wbf,
-                                                       const float* __restrict__ norm,
-                                                       const float4* __restrict__ wstat,
-                                                       float4* __restrict__ pred) {
-  __shared__ __nv_bfloat16 W[kWsParams];
-  __shared__ float N[kWsNorm];
-  for (int i = threadIdx.x; i < kWsParams; i += blockDim.x) W[i] = wbf[i];
-  for (int i = threadIdx.x; i < kWsNorm; i += blockDim.x) N[i] = norm[i];
-  __syncthreads();
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= n) return;
-  const float* f = feat + (size_t)v * kWsRow;
-  if (!(f[23] > 0.0f)) {
-    pred[v] = make_float4(0.f, 0.f, 0.f, 0.f);
-    return;
-  }
-  // the network acts on normalised features; normalising in fp32 here keeps
-  // the bf16 weights well conditioned
-  float x[kWsIn];
-#pragma unroll
-  for (int i = 0; i < kWsIn; ++i) x[i] = (f[i] - N[i]) * N[kWsIn + i];
-  const __nv_bfloat16* W1 = W + kWsW1;
-  const __nv_bfloat16* B1 = W + kWsB1;
-  const __nv_bfloat16* W2 = W + kWsW2;
-  const __nv_bfloat16* B2 = W + kWsB2;
-  const __nv_bfloat16* W3 = W + kWsW3;
-  const __nv_bfloat16* B3 = W + kWsB3;
-  float h1[kWsHidden];
-#pragma unroll
-  for (int j = 0; j < kWsHidden; ++j) {
-    float a = __bfloat162float(B1[j]);
-#pragma unroll
-    for (int i = 0; i < kWsIn; ++i) a += __bfloat162float(W1[j * kWsIn + i]) * x[i];
-    h1[j] = silu(a);
-  }
-  float o0 = __bfloat162float(B3[0]), o1 = __bfloat162float(B3[1]),
-        o2 = __bfloat162float(B3[2]);
-  for (int j = 0; j < kWsHidden; ++j) {
-    float a = __bfloat162float(B2[j]);
-#pragma unroll
-    for (int i = 0; i < kWsHidden; ++i) a += __bfloat162float(W2[j * kWsHidden + i]) * h1[i];
-    const float s = silu(a);
-    o0 += __bfloat162float(W3[j]) * s;
-    o1 += __bfloat162float(W3[kWsHidden + j]) * s;
-    o2 += __bfloat162float(W3[2 * kWsHidden + j]) * s;
-  }
-  const float* sy = N + 2 * kWsIn;
-  const float* my = sy + kWsOut;
-  const float h = wstat[v].x * f[22];
-  pred[v] = make_float4((o0 * sy[0] + my[0]) * h, (o1 * sy[1] + my[1]) * h,
-                        (o2 * sy[2] + my[2]) * h, 1.0f);
 }
 
 // ---------------------------------------------------------------------------
@@ -380,14 +321,6 @@ cudaError_t launch_ws_targets(bool state64, const DevMesh& m, const float* feat,
     ws_targets_kernel<double><<<nblk(n, 256), 256, 0, s>>>(m, feat, target);
   else
     ws_targets_kernel<float><<<nblk(n, 256), 256, 0, s>>>(m, feat, target);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_ws_infer(const float* feat, int n, const void* wbf, const float* norm,
-                            const float4* wstat, float4* pred, cudaStream_t s) {
-  if (n <= 0) return cudaSuccess;
-  ws_infer_kernel<<<nblk(n, 256), 256, 0, s>>>(
-      feat, n, static_cast<const __nv_bfloat16*>(wbf), norm, wstat, pred);
   return cudaGetLastError();
 }
 

@@ -28,8 +28,9 @@ cudaError_t launch_ws_features(int prec, int tpv, const DevMesh& m, int n_chunks
                                const double* g, int history, float* feat, cudaStream_t s);
 cudaError_t launch_ws_targets(bool state64, const DevMesh& m, const float* feat, float* target,
                               cudaStream_t s);
+// tensor-core inference (vbd_ws_tc.cu); *err is OR-ed with 1 if a wait ran out
 cudaError_t launch_ws_infer(const float* feat, int n, const void* wbf, const float* norm,
-                            const float4* wstat, float4* pred, cudaStream_t s);
+                            const float4* wstat, float4* pred, unsigned* err, cudaStream_t s);
 cudaError_t launch_to_bf16(const float* P, void* out, int n, cudaStream_t s);
 cudaError_t launch_mlp_train_batch(const float* X, const float* Y, const int* idx, int batch,
                                    const float* P, float* grad, float* scratch, double* loss,
