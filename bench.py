@@ -423,6 +423,18 @@ def run_ours(args, envs, desc, batched):
             "vertex_updates_per_s": csolved * float(cit.sum()) / t,
             "roofline_frac": cb * float(cit.sum()) / t / 1e9 / peak}
         cs.close()
+        # the same cantilever with the learned warm start (persistent mode)
+        from warpvbd_b200 import warmstart
+        ws_ = make_solver([cant], False, local, warm=warmstart.load(),
+                          tuned=tuned_config([cant], False, local, "auto", not args.no_tune))
+        wms, wit, _ = timed_steps(ws_, False, args.secondary_steps, 3, local, flush)
+        tw = float(wms.sum()) * 1e-3
+        line["cantilever160_warm_start"] = {
+            "sim_s_per_wall_s": args.secondary_steps * DT / tw,
+            "ms_per_step": 1e3 * tw / args.secondary_steps,
+            "iters_per_step": float(wit.mean()),
+            "speedup_vs_plain": t / tw}
+        ws_.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

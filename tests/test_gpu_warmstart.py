@@ -199,3 +199,49 @@ def test_trained_network_reduces_sweeps():
     print("tip error vs converged FP64, plain:       ", np.array(rel_p))
     assert it_w[5:].mean() < 0.75 * it_p[5:].mean()
     assert max(rel_w) < 5e-2 and np.median(rel_w) < 1e-2, rel_w
+
+
+def _single(s, **kw):
+    from warpvbd_b200 import VBDSolver
+    return VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000,
+                     mode="persist", **kw)
+
+
+def test_persistent_mode_rejected_prediction_reproduces_plain_vbd_exactly():
+    """The persistent kernel's warm stage (grid-wide energies, deterministic
+    partial sums): a network that only raises the potential must leave the
+    trajectory bit-identical to plain persistent VBD."""
+    s = scenes.cantilever(40)
+    plain, warm = _single(s), _single(s)
+    bad = np.random.default_rng(0).normal(scale=50.0, size=ws.N_PARAMS).astype(np.float32)
+    warm.set_warmstart(bad)
+    for _ in range(10):
+        a = plain.step(plain.old_positions, 1e-3).numpy()
+        b = warm.step(warm.old_positions, 1e-3).numpy()
+        assert plain.last_iterations == warm.last_iterations
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("n", [40, 80])
+def test_persistent_mode_trained_network_reduces_sweeps(n):
+    """A held-out cantilever (E = 1 MPa) stepped in persistent mode with and
+    without the learned warm start; both tip displacements are compared with
+    an FP64 solve to tol 1e-11 (same bounds as the batched ablation)."""
+    s = scenes.cantilever(n)
+    plain, warm = _single(s), _single(s)
+    warm.set_warmstart(_trained())
+    truth = _single(s, precision="fp64")
+    it_p, it_w = [], []
+    for k in range(30):
+        xp = plain.step(plain.old_positions, 1e-3).numpy()
+        xw = warm.step(warm.old_positions, 1e-3).numpy()
+        xt = truth.step(truth.old_positions, 1e-3, dx_tol=1e-11, max_iter=20000).numpy()
+        it_p.append(plain.last_iterations)
+        it_w.append(warm.last_iterations)
+    dt_ = (xt[s.tip] - s.vertices[s.tip]).mean(0)
+    rel_w = np.linalg.norm((xw[s.tip] - s.vertices[s.tip]).mean(0) - dt_) / np.linalg.norm(dt_)
+    rel_p = np.linalg.norm((xp[s.tip] - s.vertices[s.tip]).mean(0) - dt_) / np.linalg.norm(dt_)
+    print(f"cantilever {n}: sweeps/step plain {np.mean(it_p):.2f}, warm-started "
+          f"{np.mean(it_w):.2f}; tip error vs converged FP64 plain {rel_p:.2e}, warm {rel_w:.2e}")
+    assert np.mean(it_w[5:]) < np.mean(it_p[5:])
+    assert rel_w < 5e-2

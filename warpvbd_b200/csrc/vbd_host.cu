@@ -457,6 +457,7 @@ struct vbd_solver {
   DevBuf<StepParams> d_params;
   DevBuf<LoopControl> d_ctl;
   DevBuf<PersistCtl> d_pctl;  // persistent mode
+  DevBuf<double> d_pparts;    // persistent mode: warm-start energy partial sums
   int persist_blocks = 0;
   PersistLimits wait_limits{1ll << 26, 2000000000ull};  // every grid-barrier wait
   // block-mode work map: (environment, rank, group size) per thread block
@@ -576,6 +577,7 @@ void free_solver(vbd_solver* s) {
   s->d_params.release();
   s->d_ctl.release();
   s->d_pctl.release();
+  s->d_pparts.release();
   if (s->h_iters) cudaFreeHost(s->h_iters);
   if (s->h_status) cudaFreeHost(s->h_status);
   if (s->h_params) cudaFreeHost(s->h_params);
@@ -903,6 +905,9 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     for (const ColorInfo& ci : s->L.color)
       need = std::max(need, (ci.chunk_end - ci.chunk_begin + wpb - 1) / wpb);
     s->persist_blocks = std::min(need, per_sm * sms);
+    if (!err && s->persist_blocks > 0 &&
+        bad(s->d_pparts.alloc(4 * (size_t)s->persist_blocks), "persist parts"))
+      err = 1;
     if (!err && s->persist_blocks < 1) {
       g_last_error = "persistent mode: the kernel does not fit on the device";
       err = 1;
@@ -1126,8 +1131,14 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
       }
     }
   } else if (s->mode == VBD_MODE_PERSIST) {
+    if (s->warm) {
+      CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
+                                  s->ws_history ? 1 : 0, s->d_feat.p, st));
+      CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
+                               s->d_pred.p, s->d_ws_err.p, st));
+    }
     CUDA_TRY(launch_persist(s->prec, s->material, s->tpv, s->threads, m, s->d_params.p,
-                            s->d_pctl.p, s->persist_blocks, s->wait_limits, st));
+                            s->d_pctl.p, s->persist_blocks, s->wait_limits, s->d_pparts.p, st));
   } else if (s->mode == VBD_MODE_GRAPH) {
     rc = build_graph(s);
     if (rc != VBD_OK) return rc;
@@ -1420,8 +1431,8 @@ int vbd_set_warmstart(vbd_solver* s, const float* params, const float* norm) {
     s->warm = false;
     return VBD_OK;
   }
-  if (s->mode != VBD_MODE_BLOCK)
-    return fail(VBD_ERR_UNSUPPORTED, "the learned warm start runs in block mode");
+  if (s->mode != VBD_MODE_BLOCK && s->mode != VBD_MODE_PERSIST)
+    return fail(VBD_ERR_UNSUPPORTED, "the learned warm start runs in block or persistent mode");
   for (int i = 0; i < kWsParams; ++i)
     if (!std::isfinite(params[i])) return fail(VBD_ERR_INVALID_ARG, "non-finite parameter");
   std::vector<float> nrm(kWsNorm);

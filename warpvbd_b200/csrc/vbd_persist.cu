@@ -19,6 +19,15 @@
 //             and takes the same stop decision
 //   end       grid-stride velocity update; block 0 writes sweeps and status
 //
+// With the learned warm start (StepParams::warm and a prediction in
+// DevMesh::ws_pred), between begin and the first sweep: the incremental
+// potential at the inertia guess, then at inertia guess + alpha x predicted
+// correction for alpha = 1, 1/2, 1/4 until one is lower (else back to the
+// inertia guess).  Each potential is a grid-wide sum: every block writes its
+// partial to its own slot of `parts`, and after a barrier every block adds
+// the partials in block order, so all blocks take the same decision and the
+// result does not depend on the order in which blocks finish.
+//
 // Grid barrier: one 64-bit arrival counter, zeroed before every launch;
 // barrier k is passed when the counter reaches k * gridDim.x.  Arrival is a
 // release reduction after __syncthreads + __threadfence, the wait an acquire
@@ -116,9 +125,12 @@ __device__ __forceinline__ bool grid_sync(PersistCtl* ctl, unsigned long long ta
 template <typename Real, typename SReal, int TPV, int MAT, int FMT>
 __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
                                                       const StepParams* __restrict__ pp,
-                                                      PersistCtl* ctl, PersistLimits lim) {
+                                                      PersistCtl* ctl, PersistLimits lim,
+                                                      double* __restrict__ parts) {
   using S4 = real4<SReal>;
   __shared__ unsigned long long s_red[16];
+  __shared__ double s_dsum[16];
+  __shared__ double s_total;
   __shared__ int s_ok;
   const StepConst sc = make_const(*pp);
   const double tol = pp->tol;
@@ -148,6 +160,70 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
   VBD_GRID_SYNC();
 
   unsigned stat = 0u;
+  if (pp->warm && m.ws_pred) {
+    const S4* UT = reinterpret_cast<const S4*>(m.ut) + e.vbase;
+    // grid-wide incremental potential of the current U, partial sums in
+    // parts[slot * nb + block]
+    auto grid_energy = [&](bool inertia, int slot, bool& ok) -> double {
+      double acc = 0.0;
+      for (int c = 0; c < e.ncolors; ++c) {
+        const ColorInfo ci = m.color[e.cbase + c];
+        for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
+             q += nb * nwarps)
+          acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc,
+                                                          inertia);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (lane == 0) s_dsum[warp] = acc;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int i = 0; i < nwarps; ++i) v += s_dsum[i];
+        parts[slot * nb + blockIdx.x] = v;
+      }
+      bar += nb;
+      ok = grid_sync(ctl, bar, lim, &s_ok);
+      if (ok && threadIdx.x == 0) {
+        double v = 0.0;
+        for (int b = 0; b < nb; ++b) v += __ldcg(parts + slot * nb + b);
+        s_total = v;
+      }
+      __syncthreads();
+      return s_total;
+    };
+    bool ok = true;
+    const double e0 = grid_energy(false, 0, ok);
+    bool used = false;
+    for (int trial = 0; trial < 3 && ok && !used; ++trial) {
+      const SReal alpha = SReal(1.0 / double(1 << trial));
+      for (int i = tid; i < e.nsolved; i += nthreads) {
+        const float4 d = m.ws_pred[e.vbase + i];
+        if (d.w > 0.f) {
+          S4 v = ldcg4(UT + i);
+          v.x += alpha * SReal(d.x);
+          v.y += alpha * SReal(d.y);
+          v.z += alpha * SReal(d.z);
+          U[e.vbase + i] = v;
+        }
+      }
+      bar += nb;
+      ok = grid_sync(ctl, bar, lim, &s_ok);
+      if (!ok) break;
+      const double e1 = grid_energy(true, 1 + trial, ok);
+      used = ok && e1 < e0;  // false on NaN as well
+    }
+    if (!ok) {
+      if (threadIdx.x == 0) atomicOr(m.status, kStatTimeout);
+      return;
+    }
+    if (used) {
+      stat |= kStatWarmUsed;
+    } else {
+      for (int i = tid; i < e.nsolved; i += nthreads) U[e.vbase + i] = ldcg4(UT + i);
+      VBD_GRID_SYNC();
+    }
+  }
   int it = 0;
   bool conv = false, nan = false;
   for (;;) {
@@ -231,12 +307,14 @@ struct PersistLaunch {
   const StepParams* p;
   PersistCtl* ctl;
   PersistLimits lim;
+  double* parts;
   cudaStream_t s;
   template <typename Real, typename SReal, int TPV, int MAT, int FMT>
   cudaError_t run() {
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg = persist_config(blocks, threads, s, attr);
-    return cudaLaunchKernelEx(&cfg, persist_kernel<Real, SReal, TPV, MAT, FMT>, m, p, ctl, lim);
+    return cudaLaunchKernelEx(&cfg, persist_kernel<Real, SReal, TPV, MAT, FMT>, m, p, ctl, lim,
+                              parts);
   }
 };
 
@@ -261,12 +339,12 @@ cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int thre
 
 cudaError_t launch_persist(int prec, int material, int tpv, int threads, const DevMesh& m,
                            const StepParams* p, PersistCtl* ctl, int blocks,
-                           const PersistLimits& lim, cudaStream_t s) {
+                           const PersistLimits& lim, double* parts, cudaStream_t s) {
   if (threads < 32 || threads > 512 || threads % 32 || blocks < 1) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(PersistCtl), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(m.status, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  PersistLaunch f{blocks, threads, m, p, ctl, lim, s};
+  PersistLaunch f{blocks, threads, m, p, ctl, lim, parts, s};
   return dispatch(prec, material, m.fmt, tpv, f);
 }
 

@@ -30,9 +30,10 @@ cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int thre
 // One time step: clears *ctl and m.status[0], then a cooperative launch of
 // `blocks` blocks (at most the resident count).  Writes m.iters[0] and ORs
 // the step's status bits into m.status[0]; a barrier wait that expired adds
-// kStatTimeout there.
+// kStatTimeout there.  `parts` holds 4 x blocks doubles (warm-start energy
+// partial sums; unused without a warm-start prediction).
 cudaError_t launch_persist(int prec, int material, int tpv, int threads, const DevMesh& m,
                            const StepParams* p, PersistCtl* ctl, int blocks,
-                           const PersistLimits& lim, cudaStream_t s);
+                           const PersistLimits& lim, double* parts, cudaStream_t s);
 
 }  // namespace vbd
