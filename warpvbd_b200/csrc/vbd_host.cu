@@ -752,10 +752,13 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   const size_t smem_need = (size_t)max_env_v * smem_per_vertex;
   const bool fits = smem_need <= (size_t)env_kernel_max_smem();
   if (mode == VBD_MODE_AUTO) {
+    // measured on B200 (the autotuner's results for cantilever meshes):
+    // one block, or one cluster, holding the mesh in shared memory wins up
+    // to ~2k vertices; beyond that the persistent kernel over the whole GPU
     if (s->n_env > 1)
       mode = VBD_MODE_BLOCK;
     else
-      mode = (fits && V <= 8192) ? VBD_MODE_BLOCK : VBD_MODE_GRAPH;
+      mode = (fits && V <= 2048) ? VBD_MODE_BLOCK : VBD_MODE_PERSIST;
   }
   if (mode == VBD_MODE_BLOCK && !fits) {
     delete s;
@@ -778,10 +781,11 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     delete s;
     return fail(VBD_ERR_INVALID_ARG, "cluster size must be 1, 2, 4, 8 or 16");
   }
-  s->cluster = !block_mode ? 1 : (cl ? cl : (s->n_env > 1 ? 4 : 1));
+  s->cluster = !block_mode ? 1 : (cl ? cl : (s->n_env > 1 ? 4 : (V > 512 ? 8 : 1)));
   s->replan = block_mode && s->n_env > 1 && s->cluster > 1;
   s->tiered = s->replan && (flags & VBD_TIERED) != 0;
-  if (threads == 0) threads = block_mode ? (s->n_env > 1 ? 256 : 512) : 256;
+  if (threads == 0)
+    threads = block_mode ? (s->n_env > 1 ? 256 : 512) : (mode == VBD_MODE_PERSIST ? 128 : 256);
   if (mode == VBD_MODE_GRAPH || mode == VBD_MODE_HOSTLOOP) threads = 256;
   if (threads % 32 || threads < 32 || threads > 512) {
     delete s;
