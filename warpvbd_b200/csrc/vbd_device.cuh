@@ -207,6 +207,13 @@ __device__ __forceinline__ StepConst make_const(const StepParams& p) {
 // SmemState: packed xyz (3 values per vertex) in shared memory (block mode).
 // GlobalState: Real4 per vertex in global memory (grid mode).
 // ---------------------------------------------------------------------------
+// Byte offset of an environment's staged record table in block-mode shared
+// memory: after the packed xyz state of its nv vertices, 16-byte aligned.
+template <typename SReal>
+__host__ __device__ __forceinline__ size_t tab_smem_offset(int nv) {
+  return ((size_t)nv * 3 * sizeof(SReal) + 15) / 16 * 16;
+}
+
 template <typename SReal>
 struct SmemState {
   SReal* p;
@@ -282,7 +289,7 @@ template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
 __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const ColorInfo& ci,
                                               int q, int lane, const State& st,
                                               const StepConst& sc, unsigned long long& cmax,
-                                              unsigned& stat) {
+                                              unsigned& stat, const real4<Real>* tab) {
   using R4 = real4<Real>;
   using S4 = real4<SReal>;
   constexpr int CPW = 32 / TPV;
@@ -315,12 +322,13 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
   }
   Real g[3] = {Real(0), Real(0), Real(0)};
   Real h[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
-  const R4* tab = reinterpret_cast<const R4*>(m.rec_tab);
+  // the environment's record table: shared memory (staged by the caller) or
+  // global memory, read through the same generic pointer
   auto visit = [&](const int4& id) {
     const R4* t = tab + 3 * (size_t)id.w;
-    const R4 q0 = ldg4(t);
-    const R4 q1 = ldg4(t + 1);
-    const R4 q2 = ldg4(t + 2);
+    const R4 q0 = t[0];
+    const R4 q1 = t[1];
+    const R4 q2 = t[2];
     const S4 a = st.load(id.x);
     const S4 b = st.load(id.y);
     const S4 c = st.load(id.z);
@@ -447,7 +455,8 @@ __device__ __forceinline__ Real slot_energy(Real d0x, Real d0y, Real d0z, Real d
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
 __device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, const ColorInfo& ci,
                                                int q, int lane, const State& st,
-                                               const StepConst& sc, bool inertia) {
+                                               const StepConst& sc, bool inertia,
+                                               const real4<Real>* tab) {
   using R4 = real4<Real>;
   using S4 = real4<SReal>;
   constexpr int CPW = 32 / TPV;
@@ -464,7 +473,6 @@ __device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, cons
     uo = st.load(lv);
   }
   double acc = 0.0;
-  const R4* tab = reinterpret_cast<const R4*>(m.rec_tab);
   const size_t base = (size_t)ch.block * 32 + lane;
   for (int s = 0; s < ch.steps; ++s) {
     if (s * TPV + sub < k) {
@@ -476,7 +484,7 @@ __device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, cons
       acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
                                            Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
                                            Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
-                                           ldg4(t), ldg4(t + 1), ldg4(t + 2)));
+                                           t[0], t[1], t[2]));
     }
   }
   if (inertia && valid && sub == 0) {

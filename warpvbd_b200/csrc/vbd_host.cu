@@ -212,7 +212,7 @@ struct Layout {
   std::vector<int> new_of_old;
   std::vector<int32_t> table0;  // env 0 colour table (original ids)
   int table_colors = 0, table_max_group = 0;
-  int max_valence = 0, max_colors = 0, max_env_vertices = 0;
+  int max_valence = 0, max_colors = 0, max_env_vertices = 0, max_env_records = 0;
   long long n_slots = 0;
 };
 
@@ -376,8 +376,12 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
       for (int q = L.color[c].chunk_begin; q < L.color[c].chunk_end; ++q)
         L.chunk_owner.push_back(make_int2(c, e));
     // slot records: (n0, n1, n2, record id) per slot, the record values in a
-    // table shared by every slot with the same values in the solver precision
+    // table of this environment shared by every slot with the same values in
+    // the solver precision (record ids are environment-local, so a block can
+    // stage its environment's table in shared memory)
     L.rec_idx.resize((size_t)block_count * 32, make_int4(0, 0, 0, 0));
+    RecordTable etab;
+    etab.fp64 = L.table.fp64;
     std::vector<int> old_of_new_local(vn);
     for (int v = 0; v < vn; ++v) old_of_new_local[new_local[v]] = v;
     for (int ci_i = ei.cbase; ci_i < ei.cbase + ei.ncolors; ++ci_i) {
@@ -415,13 +419,17 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
             // strain energy, so that summing over slots counts every tet with
             // a solved vertex once (incremental-potential evaluation)
             val[11] = 1.0 / solved_in_tet;
-            const int rid = L.table.insert(val);
+            const int rid = etab.insert(val);
             L.rec_idx[blk * 32 + lane] = make_int4(ids[0], ids[1], ids[2], rid);
             L.n_slots++;
           }
         }
       }
     }
+    L.env.back().rbase = L.table.size();
+    L.env.back().nrec = etab.size();
+    L.table.vals.insert(L.table.vals.end(), etab.vals.begin(), etab.vals.end());
+    L.max_env_records = std::max(L.max_env_records, etab.size());
   }
   return VBD_OK;
 }
@@ -476,6 +484,9 @@ struct vbd_solver {
   bool tiered = false;
   int heavy_threads = 512;
   size_t smem_per_vertex = 24;
+  size_t rec_bytes = 48;      // one record: 3 Real4
+  bool tab_in_smem = false;   // kernels stage the record table in shared memory
+  size_t persist_smem = 0;    // persistent mode: bytes of the staged table
   size_t smem_heavy = 0, smem_light = 0;
   std::vector<int4> work2;
   DevBuf<int4> d_work2;
@@ -601,6 +612,13 @@ struct DeviceGuard {
   }
 };
 
+// Dynamic shared memory of a block-mode block running environment `ei`: its
+// packed xyz state, then (with_tab) its record table, 16-byte aligned.
+size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
+  const size_t state = ((size_t)ei.nv * s->smem_per_vertex + 15) / 16 * 16;
+  return with_tab ? state + (size_t)ei.nrec * s->rec_bytes : state;
+}
+
 // Block-mode work map.  Each environment's work estimate is its slot count
 // times its last sweep count (1 before the first step).  With cluster > 1 the
 // heaviest environments may each take a whole cluster (group = cluster); the
@@ -672,10 +690,10 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
 }
 
 size_t tier_smem(const vbd_solver* s, const std::vector<int4>& w) {
-  int nv = 0;
+  size_t need = 0;
   for (const int4& x : w)
-    if (x.x >= 0) nv = std::max(nv, s->L.env[x.x].nv);
-  return (size_t)nv * s->smem_per_vertex;
+    if (x.x >= 0) need = std::max(need, env_smem(s, s->L.env[x.x], s->tab_in_smem));
+  return need;
 }
 
 int upload_plan(vbd_solver* s, const int* iters) {
@@ -821,12 +839,29 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     delete s;
     return rc;
   }
-  s->smem_bytes = (size_t)s->L.max_env_vertices * smem_per_vertex;
   s->smem_per_vertex = smem_per_vertex;
+  s->rec_bytes = 3 * (s->fp64 ? 32 : 16);
+  // block mode stages each environment's record table after its state when
+  // every environment's state + table fits in a block's shared memory
+  {
+    size_t need = 0;
+    for (const EnvInfo& ei : s->L.env)
+      need = std::max(need, env_smem(s, ei, true));
+    s->tab_in_smem = block_mode && need <= (size_t)env_kernel_max_smem();
+    s->smem_bytes = 0;
+    for (const EnvInfo& ei : s->L.env)
+      s->smem_bytes = std::max(s->smem_bytes, env_smem(s, ei, s->tab_in_smem));
+    // the persistent kernel stages the mesh's table in every block if small
+    s->persist_smem = (size_t)s->L.max_env_records * s->rec_bytes;
+    if (mode == VBD_MODE_PERSIST) {
+      if (s->persist_smem > (size_t)kPersistMaxTabSmem) s->persist_smem = 0;
+      s->tab_in_smem = s->persist_smem > 0;
+    }
+  }
   s->n_records = (long long)s->L.rec_idx.size();
   // 16-bit slots when every environment-local id and record id fits
-  s->fmt = (s->L.max_env_vertices <= 65536 && s->L.table.size() <= 65536) ? kFmtIdx16
-                                                                            : kFmtIdx32;
+  s->fmt = (s->L.max_env_vertices <= 65536 && s->L.max_env_records <= 65536) ? kFmtIdx16
+                                                                              : kFmtIdx32;
 
   // ---- device upload --------------------------------------------------------
   auto bad = [&](cudaError_t e, const char* what) {
@@ -900,7 +935,8 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     // resident blocks, but no more than the largest colour can keep busy
     // (one chunk per warp): fewer blocks make cheaper grid barriers
     int per_sm = 0, sms = 0;
-    if (!err && bad(persist_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads, &per_sm),
+    if (!err && bad(persist_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads,
+                                      s->persist_smem, &per_sm),
                     "persist occupancy"))
       err = 1;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1027,6 +1063,7 @@ int set_params(vbd_solver* s, double dt, double tol, int max_iter) {
   p.max_iter = max_iter;
   p.strict_spd = (s->flags & VBD_STRICT_SPD) ? 1 : 0;
   p.warm = s->warm ? 1 : 0;
+  p.tab_in_smem = s->tab_in_smem ? 1 : 0;
   if (s->params_valid && std::memcmp(&p, &s->cur_params, sizeof p) == 0) return VBD_OK;
   // the pinned staging struct may still be read by an earlier copy
   CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -1142,7 +1179,8 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
                                s->d_pred.p, s->d_ws_err.p, st));
     }
     CUDA_TRY(launch_persist(s->prec, s->material, s->tpv, s->threads, m, s->d_params.p,
-                            s->d_pctl.p, s->persist_blocks, s->wait_limits, s->d_pparts.p, st));
+                            s->d_pctl.p, s->persist_blocks, s->wait_limits, s->d_pparts.p,
+                            s->persist_smem, st));
   } else if (s->mode == VBD_MODE_GRAPH) {
     rc = build_graph(s);
     if (rc != VBD_OK) return rc;

@@ -44,7 +44,8 @@ struct EnvInfo {
   int nsolved;  // solved vertices = local ids [0, nsolved)
   int cbase;    // first colour record in the colour table
   int ncolors;
-  int pad0, pad1;
+  int rbase;    // first record of the environment's record table (3 Real4 each)
+  int nrec;     // records of the environment (slot record ids are environment-local)
 };
 
 struct ColorInfo {
@@ -63,7 +64,7 @@ struct StepParams {
   int max_iter;
   int strict_spd;
   int warm;  // start from the learned prediction (DevMesh::ws_pred) when it lowers the energy
-  int pad;
+  int tab_in_smem;  // block mode: the launch's shared memory holds each environment's records
 };
 
 // Grid-mode loop control (one per solver).

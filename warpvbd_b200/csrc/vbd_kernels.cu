@@ -95,7 +95,7 @@ __device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, co
                                           double tol, unsigned& stat, bool& converged,
                                           unsigned long long* s_red,
                                           unsigned long long (*s_conv)[kMaxGroup],
-                                          int* s_done) {
+                                          int* s_done, const real4<Real>* tab) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   int it = 0;
   for (;;) {
@@ -103,7 +103,8 @@ __device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, co
     for (int c = 0; c < e.ncolors; ++c) {
       const ColorInfo ci = m.color[e.cbase + c];
       for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
-        process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, su, sc, cmax, stat);
+        process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, su, sc, cmax, stat,
+                                                  tab);
       group_sync<GROUP>(g);
     }
     ++it;
@@ -146,13 +147,14 @@ __device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, co
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
 __device__ double env_energy(const DevMesh& m, const EnvInfo& e, const SmemState<SReal>& st,
                              int rank, int g, const StepConst& sc, bool inertia, double* s_sum,
-                             double (*s_esum)[kMaxGroup], int buf) {
+                             double (*s_esum)[kMaxGroup], int buf, const real4<Real>* tab) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   double acc = 0.0;
   for (int c = 0; c < e.ncolors; ++c) {
     const ColorInfo ci = m.color[e.cbase + c];
     for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
-      acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, st, sc, inertia);
+      acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, st, sc, inertia,
+                                                      tab);
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -191,11 +193,12 @@ template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
 __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
                                      const SmemState<SReal>& local, int rank, int g,
                                      const StepConst& sc, double* s_sum,
-                                     double (*s_esum)[kMaxGroup]) {
+                                     double (*s_esum)[kMaxGroup], const real4<Real>* tab) {
   using S4 = real4<SReal>;
   const S4* UT = reinterpret_cast<const S4*>(m.ut) + e.vbase;
   const double e0 =
-      env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, false, s_sum, s_esum, 0);
+      env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, false, s_sum, s_esum, 0,
+                                                    tab);
   int buf = 1;
   for (int trial = 0; trial < 3; ++trial) {
     // candidate: inertia guess + alpha x prediction, formed from ut each time
@@ -212,7 +215,7 @@ __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
     }
     __syncthreads();
     const double e1 = env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, true,
-                                                                     s_sum, s_esum, buf);
+                                                                     s_sum, s_esum, buf, tab);
     buf ^= 1;
     if (e1 < e0) return (unsigned)kStatWarmUsed;  // false on NaN as well
   }
@@ -239,6 +242,17 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
   if (env < 0) return;  // padding block of a cluster of single-block environments
   const EnvInfo e = m.env[env];
   const StepConst sc = make_const(p);
+  // the environment's record table: staged in shared memory after the state
+  // when the launch reserved room for it (p.tab_in_smem), else read from
+  // global memory; either way a generic pointer to its 3 x nrec Real4
+  using R4 = real4<Real>;
+  const R4* gtab = reinterpret_cast<const R4*>(m.rec_tab) + 3 * (size_t)e.rbase;
+  const R4* tab = gtab;
+  if (p.tab_in_smem) {
+    R4* stab = reinterpret_cast<R4*>(smem_raw + tab_smem_offset<SReal>(e.nv));
+    for (int i = threadIdx.x; i < 3 * e.nrec; i += blockDim.x) stab[i] = ldg4(gtab + i);
+    tab = stab;  // visible to the block after the __syncthreads / cluster barrier below
+  }
   const double tol = tol_env ? tol_env[env] : p.tol;
   if (threadIdx.x == 0) s_stat = 0u;
   // every replica computes the inertia guess of every vertex; rank 0 writes
@@ -255,20 +269,22 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     cl.sync();  // every block of the group has started and filled its replica
     if (p.warm && m.ws_pred) {
       stat |= warm_start_stage<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, s_sum,
-                                                                 s_esum);
+                                                                 s_esum, tab);
       cl.sync();  // replicas settled before the first remote update
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, su, rank, g, sc, p.max_iter, tol,
-                                                        stat, converged, s_red, s_conv, &s_done);
+                                                        stat, converged, s_red, s_conv, &s_done,
+                                                        tab);
   } else {
     __syncthreads();
     if (p.warm && m.ws_pred) {
       stat |= warm_start_stage<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, s_sum,
-                                                                 s_esum);
+                                                                 s_esum, tab);
       __syncthreads();
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, p.max_iter, tol,
-                                                        stat, converged, s_red, s_conv, &s_done);
+                                                        stat, converged, s_red, s_conv, &s_done,
+                                                        tab);
   }
   // velocity update and write-back, vertices split over the group
   for (int i = rank + g * threadIdx.x; i < e.nv; i += g * blockDim.x) {
@@ -324,7 +340,8 @@ __global__ void __launch_bounds__(256) color_kernel(DevMesh m, int color,
   unsigned stat = 0u;
   const GlobalState<SReal> state{reinterpret_cast<S4*>(m.u)};
   if (q < ci.chunk_end)
-    process_chunk<Real, SReal, TPV, MAT, FMT>(m, 0, ci, q, lane, state, sc, cmax, stat);
+    process_chunk<Real, SReal, TPV, MAT, FMT>(m, 0, ci, q, lane, state, sc, cmax, stat,
+                                              reinterpret_cast<const real4<Real>*>(m.rec_tab));
   cmax = warp_max_u64(cmax);
   const unsigned st = __reduce_or_sync(0xffffffffu, stat);
   if (lane == 0) {

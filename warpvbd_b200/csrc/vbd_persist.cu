@@ -144,6 +144,17 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
   S4* U = reinterpret_cast<S4*>(m.u);
   const CoherentState<SReal> state{U};
   unsigned long long bar = 0ull;  // arrivals that complete the next barrier
+  // the mesh's record table: staged in this block's shared memory when the
+  // launch reserved room for it (visible after the first barrier), else read
+  // from global memory
+  using R4 = real4<Real>;
+  extern __shared__ __align__(16) unsigned char psmem[];
+  const R4* tab = reinterpret_cast<const R4*>(m.rec_tab);
+  if (pp->tab_in_smem) {
+    R4* stab = reinterpret_cast<R4*>(psmem);
+    for (int i = threadIdx.x; i < 3 * e.nrec; i += blockDim.x) stab[i] = ldg4(tab + i);
+    tab = stab;
+  }
 
 #define VBD_GRID_SYNC()                                       \
   do {                                                        \
@@ -171,7 +182,7 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
         for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
              q += nb * nwarps)
           acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc,
-                                                          inertia);
+                                                          inertia, tab);
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -235,12 +246,12 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
       if (local) {
         if (blockIdx.x == 0 && warp < nch)
           process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, ci.chunk_begin + warp, lane,
-                                                    state, sc, cmax, stat);
+                                                    state, sc, cmax, stat, tab);
       } else {
         for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
              q += nb * nwarps)
           process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, cmax,
-                                                    stat);
+                                                    stat, tab);
       }
       if (c + 1 == e.ncolors) break;
       const ColorInfo cn = m.color[e.cbase + c + 1];
@@ -287,18 +298,33 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
 #undef VBD_GRID_SYNC
 }
 
-cudaLaunchConfig_t persist_config(int blocks, int threads, cudaStream_t s,
+cudaLaunchConfig_t persist_config(int blocks, int threads, size_t smem, cudaStream_t s,
                                   cudaLaunchAttribute* attr) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(threads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cfg;
+}
+
+// The staged record table may exceed the default 48 KB of dynamic shared
+// memory: raise the kernel's limit once per device.
+template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+cudaError_t configure() {
+  static int configured_device = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (configured_device == dev) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(persist_kernel<Real, SReal, TPV, MAT, FMT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kPersistMaxTabSmem);
+  if (e == cudaSuccess) configured_device = dev;
+  return e;
 }
 
 struct PersistLaunch {
@@ -308,11 +334,14 @@ struct PersistLaunch {
   PersistCtl* ctl;
   PersistLimits lim;
   double* parts;
+  size_t smem;
   cudaStream_t s;
   template <typename Real, typename SReal, int TPV, int MAT, int FMT>
   cudaError_t run() {
+    cudaError_t e = configure<Real, SReal, TPV, MAT, FMT>();
+    if (e != cudaSuccess) return e;
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = persist_config(blocks, threads, s, attr);
+    cudaLaunchConfig_t cfg = persist_config(blocks, threads, smem, s, attr);
     return cudaLaunchKernelEx(&cfg, persist_kernel<Real, SReal, TPV, MAT, FMT>, m, p, ctl, lim,
                               parts);
   }
@@ -320,31 +349,36 @@ struct PersistLaunch {
 
 struct PersistOccupancy {
   int threads;
+  size_t smem;
   int* out;
   template <typename Real, typename SReal, int TPV, int MAT, int FMT>
   cudaError_t run() {
+    cudaError_t e = configure<Real, SReal, TPV, MAT, FMT>();
+    if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        out, persist_kernel<Real, SReal, TPV, MAT, FMT>, threads, 0);
+        out, persist_kernel<Real, SReal, TPV, MAT, FMT>, threads, smem);
   }
 };
 
 }  // namespace
 
-cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int threads,
+cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int threads, size_t smem,
                               int* blocks_per_sm) {
   if (threads < 32 || threads > 512 || threads % 32) return cudaErrorInvalidValue;
-  PersistOccupancy f{threads, blocks_per_sm};
+  PersistOccupancy f{threads, smem, blocks_per_sm};
   return dispatch(prec, material, fmt, tpv, f);
 }
 
 cudaError_t launch_persist(int prec, int material, int tpv, int threads, const DevMesh& m,
                            const StepParams* p, PersistCtl* ctl, int blocks,
-                           const PersistLimits& lim, double* parts, cudaStream_t s) {
+                           const PersistLimits& lim, double* parts, size_t smem,
+                           cudaStream_t s) {
   if (threads < 32 || threads > 512 || threads % 32 || blocks < 1) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(PersistCtl), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(m.status, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  PersistLaunch f{blocks, threads, m, p, ctl, lim, parts, s};
+  if (smem > (size_t)kPersistMaxTabSmem) return cudaErrorInvalidValue;
+  PersistLaunch f{blocks, threads, m, p, ctl, lim, parts, smem, s};
   return dispatch(prec, material, m.fmt, tpv, f);
 }
 

@@ -23,17 +23,23 @@ struct PersistLimits {
   unsigned long long max_wait_ns;  // wall-clock limit
 };
 
-// Resident persist_kernel blocks per SM for `threads` threads.
-cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int threads,
+// Largest record table (bytes) a persistent launch stages in shared memory.
+constexpr int kPersistMaxTabSmem = 64 * 1024;
+
+// Resident persist_kernel blocks per SM for `threads` threads and `smem`
+// bytes of dynamic shared memory (the staged record table, or 0).
+cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int threads, size_t smem,
                               int* blocks_per_sm);
 
 // One time step: clears *ctl and m.status[0], then a cooperative launch of
 // `blocks` blocks (at most the resident count).  Writes m.iters[0] and ORs
 // the step's status bits into m.status[0]; a barrier wait that expired adds
 // kStatTimeout there.  `parts` holds 4 x blocks doubles (warm-start energy
-// partial sums; unused without a warm-start prediction).
+// partial sums; unused without a warm-start prediction).  `smem`: bytes of the
+// record table when StepParams::tab_in_smem stages it, else 0.
 cudaError_t launch_persist(int prec, int material, int tpv, int threads, const DevMesh& m,
                            const StepParams* p, PersistCtl* ctl, int blocks,
-                           const PersistLimits& lim, double* parts, cudaStream_t s);
+                           const PersistLimits& lim, double* parts, size_t smem,
+                           cudaStream_t s);
 
 }  // namespace vbd
