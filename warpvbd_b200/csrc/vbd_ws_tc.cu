@@ -25,9 +25,13 @@
 // byte offset) and consecutive 8-row groups 128 bytes apart (stride byte
 // offset).
 //
-// TMEM: 128 columns per CTA.  The dynamic shared memory request (60 KB) lets
-// at most 3 CTAs share an SM, so the 512 TMEM columns of an SM always
-// suffice and tcgen05.alloc never waits.
+// TMEM: 128 columns per CTA.  The dynamic shared memory request (48 KB, plus
+// the 1 KB the driver reserves per CTA) lets at most 4 CTAs share an SM, so
+// the 512 TMEM columns of an SM always suffice and tcgen05.alloc never waits.
+//
+// Each thread prefetches its row of the CTA's next tile into registers while
+// the current tile's two MMA rounds run, so the feature loads (the kernel's
+// only HBM traffic besides the predictions) overlap the tensor-core work.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -51,9 +55,12 @@ constexpr int kOffF = kOffA2 + kTileM * kWsHidden * 2;      // fp32 constants
 constexpr int kNF = 64 + 64 + 3 * 64 + 4 + kWsNorm + 2;     // b1 b2 W3 b3 norm (padded)
 constexpr int kOffBar = (kOffF + kNF * 4 + 15) / 16 * 16;   // mbarrier (8 B) + TMEM address
 constexpr int kSmemUsed = kOffBar + 16;
-constexpr int kSmemRequest = 60 * 1024;  // caps residency at 3 CTAs per SM
+constexpr int kSmemRequest = 48 * 1024;  // caps residency at 4 CTAs per SM
+constexpr int kCtasPerSm = 4;
 static_assert(kSmemUsed <= kSmemRequest, "shared-memory map exceeds the request");
-static_assert(4 * kSmemRequest > 228 * 1024, "request must keep CTAs per SM <= 3");
+static_assert((kCtasPerSm + 1) * (kSmemRequest + 1024) > 228 * 1024,
+              "the request must keep CTAs per SM <= 4 (TMEM: 4 x 128 columns)");
+static_assert(kCtasPerSm * kTmemCols <= 512, "TMEM columns per SM");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -154,7 +161,19 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
   for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float silu_f(float a) { return a / (1.0f + __expf(-a)); }
+// SiLU from the identity x sigma(x) = x/2 (1 + tanh(x/2)), with the
+// hardware tanh approximation (PTX tanh.approx.f32, one special-function
+// operation instead of an exponential and a reciprocal); its error, ~2^-11
+// relative, is below the bf16 rounding the activations get next.
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float silu_f(float a) {
+  const float h = 0.5f * a;
+  return fmaf(h, tanh_approx(h), h);
+}
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   const __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
@@ -237,36 +256,39 @@ __global__ void __launch_bounds__(128) ws_infer_tc_kernel(const float* __restric
   bool ok = true;
 
   const int tiles = (n + kTileM - 1) / kTileM;
+  // this thread's feature row of a tile (zeros past the end)
+  auto load_row = [&](int tile, float4* r) {
+    const int v = tile * kTileM + tid;
+    if (tile < tiles && v < n) {
+      const float4* f4 = reinterpret_cast<const float4*>(feat + (size_t)v * kWsRow);
+#pragma unroll
+      for (int q = 0; q < kWsRow / 4; ++q) r[q] = __ldg(f4 + q);
+    } else {
+#pragma unroll
+      for (int q = 0; q < kWsRow / 4; ++q) r[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  float4 row[kWsRow / 4];
+  load_row(blockIdx.x, row);
   for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
     const int v = tile * kTileM + tid;
     const bool in = v < n;
-    float f22 = 0.0f, f23 = 0.0f;
+    const float f22 = row[5].z, f23 = row[5].w;
     {
       // this thread's row of A1: normalised inputs in bf16, zero padded
+      const float* f = reinterpret_cast<const float*>(row);
       float x[kK1];
 #pragma unroll
       for (int i = 0; i < kK1; ++i) x[i] = 0.0f;
-      if (in) {
-        const float4* f4 = reinterpret_cast<const float4*>(feat + (size_t)v * kWsRow);
-        float f[kWsRow];
+      if (in && f23 > 0.0f) {
 #pragma unroll
-        for (int q = 0; q < kWsRow / 4; ++q) {
-          const float4 t = __ldg(f4 + q);
-          f[4 * q] = t.x;
-          f[4 * q + 1] = t.y;
-          f[4 * q + 2] = t.z;
-          f[4 * q + 3] = t.w;
-        }
-        f22 = f[22];
-        f23 = f[23];
-        if (f23 > 0.0f) {
-#pragma unroll
-          for (int i = 0; i < kWsIn; ++i) x[i] = (f[i] - sN[i]) * sN[kWsIn + i];
-        }
+        for (int i = 0; i < kWsIn; ++i) x[i] = (f[i] - sN[i]) * sN[kWsIn + i];
       }
 #pragma unroll
       for (int k0 = 0; k0 < kK1; k0 += 8) store8(A1, kTileM, tid, k0, x + k0);
     }
+    // the next tile's row, in flight during this tile's MMAs
+    load_row(tile + gridDim.x, row);
     fence_proxy_async();
     tc_fence_before();
     __syncthreads();
@@ -367,7 +389,7 @@ cudaError_t launch_ws_infer(const float* feat, int n, const void* wbf, const flo
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int tiles = (n + kTileM - 1) / kTileM;
-  const int grid = tiles < 3 * sms ? tiles : 3 * sms;
+  const int grid = tiles < kCtasPerSm * sms ? tiles : kCtasPerSm * sms;
   ws_infer_tc_kernel<<<grid, kTileM, kSmemRequest, s>>>(
       feat, n, static_cast<const __nv_bfloat16*>(wbf), norm, wstat, pred, err, 1 << 22);
   return cudaGetLastError();
