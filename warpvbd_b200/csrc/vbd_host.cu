@@ -496,6 +496,7 @@ struct vbd_solver {
   DevBuf<float4> d_wstat;
   DevBuf<int2> d_chunk_owner;
   DevBuf<float> d_feat;           // [V][24], allocated on first use
+  DevBuf<float> d_wpack;          // [V][6] packed fp32 displacement / velocity (features)
   DevBuf<float4> d_pred;          // [V]
   DevBuf<unsigned char> d_wbf;    // bf16 network parameters
   DevBuf<float> d_wparams;        // fp32 staging for the conversion
@@ -580,6 +581,7 @@ void free_solver(vbd_solver* s) {
   s->d_wstat.release();
   s->d_chunk_owner.release();
   s->d_feat.release();
+  s->d_wpack.release();
   s->d_pred.release();
   s->d_wbf.release();
   s->d_wparams.release();
@@ -1143,7 +1145,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
     if (s->warm) {
       // features of the coming step, then the network's predicted corrections
       CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
-                                  s->ws_history ? 1 : 0, s->d_feat.p, st));
+                                  s->ws_history ? 1 : 0, s->d_wpack.p, s->d_feat.p, st));
       CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
                                s->d_pred.p, s->d_ws_err.p, st));
     }
@@ -1174,7 +1176,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
   } else if (s->mode == VBD_MODE_PERSIST) {
     if (s->warm) {
       CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
-                                  s->ws_history ? 1 : 0, s->d_feat.p, st));
+                                  s->ws_history ? 1 : 0, s->d_wpack.p, s->d_feat.p, st));
       CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
                                s->d_pred.p, s->d_ws_err.p, st));
     }
@@ -1463,6 +1465,7 @@ static int ensure_ws_buffers(vbd_solver* s) {
     CUDA_TRY(cudaMemsetAsync(s->d_feat.p, 0, sizeof(float) * (size_t)s->V * kWsRow, s->stream));
   }
   if (!s->d_pred.p) CUDA_TRY(s->d_pred.alloc((size_t)s->V));
+  if (!s->d_wpack.p) CUDA_TRY(s->d_wpack.alloc(6 * (size_t)s->V));
   return VBD_OK;
 }
 
@@ -1510,7 +1513,7 @@ int vbd_ws_features(vbd_solver* s, double dt, float* features) {
   if (rc != VBD_OK) return rc;
   CUDA_TRY(cudaMemsetAsync(features, 0, sizeof(float) * (size_t)s->V * kWsRow, s->stream));
   CUDA_TRY(launch_ws_features(s->prec, s->tpv, s->mesh(), (int)s->L.chunk.size(), dt, s->g,
-                              s->ws_history ? 1 : 0, features, s->stream));
+                              s->ws_history ? 1 : 0, s->d_wpack.p, features, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
   return VBD_OK;
 }

@@ -45,12 +45,30 @@ __device__ __forceinline__ float silu_grad(float a) {
 }
 
 // ---------------------------------------------------------------------------
-// Features: one warp per chunk, TPV lanes per vertex walk its slots.
+// Features: one warp per chunk, TPV lanes per vertex walk its slots.  The
+// neighbour sums read a packed fp32 copy of every vertex's displacement and
+// velocity (24 B instead of two 32 B double4 per neighbour visit, written
+// once per step by ws_pack_kernel); the vertex's own values stay in the
+// state precision.  fp32 differences of neighbouring displacements are far
+// more accurate than the bf16 the network's inputs are rounded to.
 // ---------------------------------------------------------------------------
+template <typename SReal>
+__global__ void ws_pack_kernel(DevMesh m, float4* __restrict__ pa, float2* __restrict__ pb) {
+  using S4 = real4<SReal>;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.n_vertices) return;
+  const S4 u = reinterpret_cast<const S4*>(m.u)[i];
+  const S4 v = reinterpret_cast<const S4*>(m.vel)[i];
+  pa[i] = make_float4(float(u.x), float(u.y), float(u.z), float(v.x));
+  pb[i] = make_float2(float(v.y), float(v.z));
+}
+
 template <typename SReal, int TPV, int FMT>
 __global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunks, double dt,
                                                           double gx, double gy, double gz,
-                                                          int history, float* __restrict__ feat) {
+                                                          int history, const float4* __restrict__ pa,
+                                                          const float2* __restrict__ pb,
+                                                          float* __restrict__ feat) {
   using S4 = real4<SReal>;
   const int lane = threadIdx.x & 31;
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -74,7 +92,9 @@ __global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunk
     uo = U[gv];
     vo = VEL[gv];
   }
-  double su[3] = {0.0, 0.0, 0.0}, sv[3] = {0.0, 0.0, 0.0};
+  float su[3] = {0.f, 0.f, 0.f}, sv[3] = {0.f, 0.f, 0.f};
+  const float ux = float(uo.x), uy = float(uo.y), uz = float(uo.z);
+  const float vx = float(vo.x), vy = float(vo.y), vz = float(vo.z);
   const size_t base = (size_t)ch.block * 32 + lane;
   for (int s = 0; s < ch.steps; ++s) {
     if (s * TPV + sub < k) {
@@ -82,14 +102,14 @@ __global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunk
       const int nb[3] = {id.x, id.y, id.z};
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const S4 a = U[vbase + nb[j]];
-        const S4 b = VEL[vbase + nb[j]];
-        su[0] += double(a.x - uo.x);
-        su[1] += double(a.y - uo.y);
-        su[2] += double(a.z - uo.z);
-        sv[0] += double(b.x - vo.x);
-        sv[1] += double(b.y - vo.y);
-        sv[2] += double(b.z - vo.z);
+        const float4 a = __ldg(pa + vbase + nb[j]);
+        const float2 b = __ldg(pb + vbase + nb[j]);
+        su[0] += a.x - ux;
+        su[1] += a.y - uy;
+        su[2] += a.z - uz;
+        sv[0] += a.w - vx;
+        sv[1] += b.x - vy;
+        sv[2] += b.y - vz;
       }
     }
   }
@@ -292,14 +312,18 @@ struct FeatLaunch {
   int n_chunks;
   double dt, gx, gy, gz;
   int history;
+  float* pack;
   float* feat;
   cudaStream_t s;
   template <typename Real, typename SReal, int TPV, int MAT, int FMT>
   cudaError_t run() {
     const int blocks = (n_chunks + 7) / 8;
     if (blocks == 0) return cudaSuccess;
+    float4* pa = reinterpret_cast<float4*>(pack);
+    float2* pb = reinterpret_cast<float2*>(pack + 4 * (size_t)m.n_vertices);
+    ws_pack_kernel<SReal><<<(m.n_vertices + 255) / 256, 256, 0, s>>>(m, pa, pb);
     ws_features_kernel<SReal, TPV, FMT><<<blocks, 256, 0, s>>>(m, n_chunks, dt, gx, gy, gz,
-                                                               history, feat);
+                                                               history, pa, pb, feat);
     return cudaGetLastError();
   }
 };
@@ -307,8 +331,9 @@ inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
 }  // namespace
 
 cudaError_t launch_ws_features(int prec, int tpv, const DevMesh& m, int n_chunks, double dt,
-                               const double* g, int history, float* feat, cudaStream_t s) {
-  FeatLaunch f{m, n_chunks, dt, g[0], g[1], g[2], history, feat, s};
+                               const double* g, int history, float* pack, float* feat,
+                               cudaStream_t s) {
+  FeatLaunch f{m, n_chunks, dt, g[0], g[1], g[2], history, pack, feat, s};
   // the features depend on the state precision only; material is irrelevant
   return dispatch(prec, kSNH, m.fmt, tpv, f);
 }

@@ -24,8 +24,11 @@ constexpr int kWsNorm = 2 * kWsIn + 2 * kWsOut;  // 50
 // floats of training scratch per minibatch sample: A1, A2, D1, D2, dOut
 constexpr int kWsScratchPerSample = 4 * kWsHidden + kWsOut;
 
+// `pack`: scratch of 6 floats per vertex (the packed fp32 displacement and
+// velocity the neighbour sums read, rewritten by every call).
 cudaError_t launch_ws_features(int prec, int tpv, const DevMesh& m, int n_chunks, double dt,
-                               const double* g, int history, float* feat, cudaStream_t s);
+                               const double* g, int history, float* pack, float* feat,
+                               cudaStream_t s);
 cudaError_t launch_ws_targets(bool state64, const DevMesh& m, const float* feat, float* target,
                               cudaStream_t s);
 // tensor-core inference (vbd_ws_tc.cu); *err is OR-ed with 1 if a wait ran out
