@@ -318,9 +318,10 @@ def run_ours(args, envs, desc, batched):
     slots = np.array([p[2] for p in per_env])
     solved = np.array([p[1] for p in per_env])
     mode = MODE_NAMES[info["mode"]]
-    # sweeps, plus the two energy passes over every slot when the warm start
-    # compares the prediction with the inertia guess
-    passes = iters + (2 if warm is not None else 0)
+    # sweeps, plus the energy pass over every slot (both potentials in one
+    # pass) when the warm start compares the prediction with the inertia
+    # guess; the rare extra passes of the line search are not counted
+    passes = iters + (1 if warm is not None else 0)
     alg_bytes = float((passes * b_sweep[None, :]).sum())
     achieved = alg_bytes / (total_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
@@ -382,7 +383,7 @@ def run_ours(args, envs, desc, batched):
             t = torch.tensor([pt], device=f"cuda:{local}")
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             pt = float(t.item())
-        ppass = pit + (2 if other is not None else 0)
+        ppass = pit + (1 if other is not None else 0)
         pbytes = float((ppass * b_sweep[None, :]).sum())
         pv = world * n_env * args.steps * DT / (pt * 1e-3)
         key = "warm_start_batched" if other is not None else "plain_batched"

@@ -495,6 +495,73 @@ __device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, cons
   return acc;
 }
 
+// Both potentials the learned warm start compares, in one pass over the
+// slots: (x) the elastic energy of the current state (the inertia guess, whose
+// inertia term is zero) and (y) the incremental potential of the state shifted
+// by the predicted correction (DevMesh::ws_pred, where w > 0), inertia term
+// included.  The shifted positions are formed exactly as the warm-start stage
+// stores them (state + correction in the state precision), so (y) equals the
+// potential a separate pass over the shifted state would give, bit for bit.
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
+__device__ __forceinline__ double2 energy_chunk_pair(const DevMesh& m, int vbase,
+                                                     const ColorInfo& ci, int q, int lane,
+                                                     const State& st, const StepConst& sc,
+                                                     const real4<Real>* tab) {
+  using R4 = real4<Real>;
+  using S4 = real4<SReal>;
+  constexpr int CPW = 32 / TPV;
+  const int vi = lane / TPV, sub = lane % TPV;
+  const int gv = ci.vbegin + (q - ci.chunk_begin) * CPW + vi;
+  const bool valid = gv < ci.vend;
+  const int lv = gv - vbase;
+  const ChunkInfo ch = m.chunk[q];
+  auto shifted = [&](S4 v, int local_id) {
+    const float4 d = m.ws_pred[vbase + local_id];
+    if (d.w > 0.f) {
+      v.x += SReal(d.x);
+      v.y += SReal(d.y);
+      v.z += SReal(d.z);
+    }
+    return v;
+  };
+  int k = 0;
+  S4 uo, uob;
+  uo.x = uo.y = uo.z = uo.w = SReal(0);
+  uob = uo;
+  if (valid) {
+    k = __ldg(m.valence + gv);
+    uo = st.load(lv);
+    uob = shifted(uo, lv);
+  }
+  double acc = 0.0, accb = 0.0;
+  const size_t base = (size_t)ch.block * 32 + lane;
+  for (int s = 0; s < ch.steps; ++s) {
+    if (s * TPV + sub < k) {
+      const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
+      const R4* t = tab + 3 * (size_t)id.w;
+      const R4 q0 = t[0], q1 = t[1], q2 = t[2];
+      const S4 a = st.load(id.x);
+      const S4 b = st.load(id.y);
+      const S4 c = st.load(id.z);
+      acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                                           Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                                           Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
+                                           q0, q1, q2));
+      const S4 ab = shifted(a, id.x), bb = shifted(b, id.y), cb = shifted(c, id.z);
+      accb += double(slot_energy<Real, MAT>(
+          Real(ab.x - uob.x), Real(ab.y - uob.y), Real(ab.z - uob.z), Real(bb.x - uob.x),
+          Real(bb.y - uob.y), Real(bb.z - uob.z), Real(cb.x - uob.x), Real(cb.y - uob.y),
+          Real(cb.z - uob.z), q0, q1, q2));
+    }
+  }
+  if (valid && sub == 0) {
+    const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
+    const double dx = double(uob.x - tt.x), dy = double(uob.y - tt.y), dz = double(uob.z - tt.z);
+    accb += 0.5 * double(tt.w) * sc.inv_dt2 * (dx * dx + dy * dy + dz * dz);
+  }
+  return make_double2(acc, accb);
+}
+
 // Inertia target and initial guess (position_initialization,
 // vbd_solver.py:277-292): ut = u + dt v + dt^2 g (w keeps the lumped mass),
 // up = u (written when write_back), and active vertices start from ut.

@@ -182,27 +182,84 @@ __device__ double env_energy(const DevMesh& m, const EnvInfo& e, const SmemState
   return v;
 }
 
+// Both potentials of energy_chunk_pair summed over the environment (and the
+// group): x = at the inertia guess, y = at inertia guess + predicted
+// correction.  Block sums are exchanged through distributed shared memory in
+// s_pair (one slot per rank).
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
+__device__ double2 env_energy_pair(const DevMesh& m, const EnvInfo& e, const SmemState<SReal>& st,
+                                   int rank, int g, const StepConst& sc, double* s_sum,
+                                   double2* s_pair, const real4<Real>* tab) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  double a = 0.0, b = 0.0;
+  for (int c = 0; c < e.ncolors; ++c) {
+    const ColorInfo ci = m.color[e.cbase + c];
+    for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps) {
+      const double2 v = energy_chunk_pair<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, st,
+                                                                       sc, tab);
+      a += v.x;
+      b += v.y;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, off);
+    b += __shfl_xor_sync(0xffffffffu, b, off);
+  }
+  // s_sum[0..15] and [16..31] hold the warps' two sums (at most 16 warps)
+  if (lane == 0) {
+    s_sum[warp] = a;
+    s_sum[16 + warp] = b;
+  }
+  __syncthreads();
+  __shared__ double2 s_tot;
+  if (threadIdx.x == 0) {
+    double va = 0.0, vb = 0.0;
+    for (int i = 0; i < nwarps; ++i) {
+      va += s_sum[i];
+      vb += s_sum[16 + i];
+    }
+    s_tot = make_double2(va, vb);
+  }
+  if (GROUP && g > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int r = 0; r < g; ++r) *cl.map_shared_rank(&s_pair[rank], r) = s_tot;
+    cl.sync();
+    if (threadIdx.x == 0) {
+      double va = 0.0, vb = 0.0;
+      for (int r = 0; r < g; ++r) {
+        va += s_pair[r].x;
+        vb += s_pair[r].y;
+      }
+      s_tot = make_double2(va, vb);
+    }
+  }
+  __syncthreads();
+  const double2 v = s_tot;
+  __syncthreads();  // s_sum / s_tot are reused by the next call
+  return v;
+}
+
 // Learned warm start: compare the incremental potential at the inertia guess
 // (the replica's current content) with the one at inertia guess + alpha x
 // predicted correction for alpha = 1, 1/2, 1/4 (a backtracking line search
 // along the prediction: the next alpha is tried only when the previous one
 // did not lower the potential), and keep the first that is lower, else the
-// inertia guess.  Every block of a group decides the same way from the same
-// sums.  Returns kStatWarmUsed or 0.
+// inertia guess.  The first comparison (alpha = 1) takes one pass over the
+// slots for both potentials.  Every block of a group decides the same way
+// from the same sums.  Returns kStatWarmUsed or 0.
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
 __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
                                      const SmemState<SReal>& local, int rank, int g,
                                      const StepConst& sc, double* s_sum,
-                                     double (*s_esum)[kMaxGroup], const real4<Real>* tab) {
+                                     double (*s_esum)[kMaxGroup], double2* s_pair,
+                                     const real4<Real>* tab) {
   using S4 = real4<SReal>;
   const S4* UT = reinterpret_cast<const S4*>(m.ut) + e.vbase;
-  const double e0 =
-      env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, false, s_sum, s_esum, 0,
-                                                    tab);
-  int buf = 1;
-  for (int trial = 0; trial < 3; ++trial) {
+  auto place = [&](SReal alpha) {
     // candidate: inertia guess + alpha x prediction, formed from ut each time
-    const SReal alpha = SReal(1.0 / double(1 << trial));
     for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x) {
       const float4 d = m.ws_pred[e.vbase + i];
       if (d.w > 0.f) {
@@ -213,11 +270,22 @@ __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
         local.store(i, v);
       }
     }
+  };
+  const double2 e01 = env_energy_pair<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc,
+                                                                          s_sum, s_pair, tab);
+  const double e0 = e01.x;
+  if (e01.y < e0) {  // false on NaN as well
+    place(SReal(1));
+    return (unsigned)kStatWarmUsed;
+  }
+  int buf = 0;
+  for (int trial = 1; trial < 3; ++trial) {
+    place(SReal(1.0 / double(1 << trial)));
     __syncthreads();
     const double e1 = env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, true,
                                                                      s_sum, s_esum, buf, tab);
     buf ^= 1;
-    if (e1 < e0) return (unsigned)kStatWarmUsed;  // false on NaN as well
+    if (e1 < e0) return (unsigned)kStatWarmUsed;
   }
   // back to the inertia guess, exactly as begin computed it
   for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x) local.store(i, ldcg4(UT + i));
@@ -235,6 +303,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
   __shared__ unsigned long long s_conv[2][kMaxGroup];
   __shared__ double s_sum[33];
   __shared__ double s_esum[2][kMaxGroup];
+  __shared__ double2 s_pair[kMaxGroup];
   __shared__ int s_done;
   __shared__ unsigned s_stat;
   const int4 w = work[blockIdx.x];
@@ -269,7 +338,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     cl.sync();  // every block of the group has started and filled its replica
     if (p.warm && m.ws_pred) {
       stat |= warm_start_stage<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, s_sum,
-                                                                 s_esum, tab);
+                                                                 s_esum, s_pair, tab);
       cl.sync();  // replicas settled before the first remote update
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, su, rank, g, sc, p.max_iter, tol,
@@ -279,7 +348,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     __syncthreads();
     if (p.warm && m.ws_pred) {
       stat |= warm_start_stage<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, s_sum,
-                                                                 s_esum, tab);
+                                                                 s_esum, s_pair, tab);
       __syncthreads();
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, p.max_iter, tol,
