@@ -294,21 +294,23 @@ def run_ours(args, envs, desc, batched):
     n_env = len(envs)
     value = world * n_env * args.steps * DT / (total_ms * 1e-3)
 
-    # end to end through the public API, host arrays in and out every step
+    # end to end through the public API: every step uploads the positions
+    # from page-locked host memory and downloads the new ones into it
     n_vertices = sum(e.n_vertices for e in envs)
+    xh = torch.empty((n_vertices, 3), dtype=torch.float64, pin_memory=True).numpy()
     if batched:
-        x = sol.positions()
+        sol.positions(out=xh)
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            sol.set_state(positions=x)
+            sol.set_state(positions=xh)
             sol.step(DT)
-            x = sol.positions()
+            sol.positions(out=xh)
         e2e_s = time.perf_counter() - t0
     else:
-        x = sol.old_positions.numpy()
+        sol.old_positions.numpy(out=xh)
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            x = sol.step(x, DT).numpy()
+            sol.step(xh, DT).numpy(out=xh)
         e2e_s = time.perf_counter() - t0
     e2e = world * n_env * args.e2e_steps * DT / e2e_s
 

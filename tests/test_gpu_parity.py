@@ -222,3 +222,26 @@ def test_tiered_launch_is_bit_identical_to_one_launch(cluster, threads):
         assert np.array_equal(a, b)
     assert np.array_equal(one.positions(), two.positions())
     assert np.array_equal(one.velocities(), two.velocities())
+
+
+def test_downloads_into_caller_arrays():
+    """positions(out=...) / DeviceArray.numpy(out=...) fill a caller array
+    (e.g. page-locked) with exactly what a fresh download returns."""
+    import torch
+    from warpvbd_b200 import BatchedVBDSolver, VBDSolver
+    envs = scenes.env_batch(3, seed=2)
+    b = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000)
+    b.step(1e-3)
+    n = b.n_vertices
+    pinned = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    assert b.positions(out=pinned) is pinned
+    assert np.array_equal(pinned, b.positions())
+    b.set_state(positions=pinned)
+    assert np.array_equal(b.positions(), pinned)
+    s = scenes.cantilever(20)
+    v = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000)
+    x = torch.empty((s.n_vertices, 3), dtype=torch.float64, pin_memory=True).numpy()
+    v.step(v.old_positions, 1e-3).numpy(out=x)
+    assert np.array_equal(x, v.old_positions.numpy())
+    with pytest.raises(ValueError):
+        v.old_positions.numpy(out=np.empty((3, 3)))

@@ -13,7 +13,8 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .vbd_solver import _host, _device_index, _set_warmstart, _ws_features, _ws_targets
+from .vbd_solver import (_device_index, _host, _host_out, _set_warmstart, _ws_features,
+                         _ws_targets)
 
 
 class BatchedVBDSolver:
@@ -129,13 +130,15 @@ class BatchedVBDSolver:
             raise FloatingPointError("VBD step produced non-finite positions")
         _lib.check(st, "vbd_step_batched")
 
-    def positions(self):
-        out = np.empty((self.n_vertices, 3))
+    def positions(self, out=None):
+        """float64 [V, 3]; `out`: an existing C-contiguous float64 array to fill
+        (e.g. page-locked, for fast transfers)."""
+        out = _host_out(out, self.n_vertices)
         _lib.check(_lib.load().vbd_get_positions(self._h, _lib.ptr(out, "d")))
         return out
 
-    def velocities(self):
-        out = np.empty((self.n_vertices, 3))
+    def velocities(self, out=None):
+        out = _host_out(out, self.n_vertices)
         _lib.check(_lib.load().vbd_get_velocities(self._h, _lib.ptr(out, "d")))
         return out
 

@@ -55,6 +55,16 @@ def _device_index(device):
                      "there is no CPU path")
 
 
+def _host_out(out, n):
+    """A float64 [n, 3] C-contiguous host array to download into."""
+    if out is None:
+        return np.empty((n, 3))
+    if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (n, 3)
+            or not out.flags.c_contiguous):
+        raise ValueError(f"out must be a C-contiguous float64 array of shape ({n}, 3)")
+    return out
+
+
 def _set_warmstart(handle, model):
     """Enable the learned warm start, or disable it (None).  `model` is a
     (params, norm) pair as returned by warmstart.load / train_warmstart, or
@@ -113,14 +123,19 @@ class DeviceArray:
     def __len__(self):
         return self._solver.n_vertices
 
-    def numpy(self):
+    def numpy(self, out=None):
+        """Host copy (float64 [V, 3]); `out`: an existing C-contiguous float64
+        array to fill instead (e.g. page-locked, for fast transfers)."""
         if self._host is not None:
-            return self._host.copy()
+            if out is None:
+                return self._host.copy()
+            out[...] = self._host
+            return out
         if self._version != self._solver._version:
             raise RuntimeError(
                 "this array's solver state was overwritten by a later step or reset; call "
                 ".numpy() (or .copy()) before stepping again")
-        return self._solver._download(self._kind)
+        return self._solver._download(self._kind, out)
 
     def copy(self):
         """Materialise a host snapshot that survives later steps."""
@@ -276,9 +291,9 @@ class VBDSolver:
         return _lib.load().vbd_get_stream(self._h)
 
     # ---- state --------------------------------------------------------------
-    def _download(self, kind):
+    def _download(self, kind, out=None):
         L = _lib.load()
-        out = np.empty((self.n_vertices, 3))
+        out = _host_out(out, self.n_vertices)
         fn = L.vbd_get_positions if kind == "x" else L.vbd_get_velocities
         _lib.check(fn(self._h, _lib.ptr(out, "d")), "download")
         return out
