@@ -190,7 +190,7 @@ __device__ __forceinline__ void store8(unsigned char* tile, int R, int r, int k0
   *reinterpret_cast<uint4*>(tile + canon_off(r, k0, R)) = q;
 }
 
-__global__ void __launch_bounds__(128) ws_infer_tc_kernel(const float* __restrict__ feat, int n,
+__global__ void __launch_bounds__(128, kCtasPerSm) ws_infer_tc_kernel(const float* __restrict__ feat, int n,
                                                           const __nv_bfloat16* __restrict__ wbf,
                                                           const float* __restrict__ norm,
                                                           const float4* __restrict__ wstat,
@@ -383,6 +383,11 @@ cudaError_t launch_ws_infer(const float* feat, int n, const void* wbf, const flo
   if (configured != dev) {
     cudaError_t e = cudaFuncSetAttribute(ws_infer_tc_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRequest);
+    // all of the SM's unified memory as shared memory, so that 4 CTAs fit
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ws_infer_tc_kernel,
+                               cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     configured = dev;
   }
