@@ -1,5 +1,5 @@
 // Internal layout shared by the host setup (vbd_host.cu) and the kernels
-// (vbd_kernels.cu).
+// (vbd_kernels.cu, vbd_persist.cu, vbd_noalloc.cu, vbd_warmstart.cu).
 //
 // Device data of one solver ("mesh" = one or more independent environments):
 //
@@ -11,16 +11,20 @@
 //   u, ut, up, vel   Real4 per vertex: displacement from the rest position,
 //              inertia target (w = lumped mass), displacement at step start,
 //              velocity.
-//   slots      one record per incident (vertex, tet) pair, SELL-32 layout: a
+//   slots      one per incident (vertex, tet) pair, SELL-32 layout: a
 //              "chunk" is 32 lanes = 32/TPV vertices x TPV lanes; chunk q has
-//              `steps` blocks of 32 records, block b holds, for lane l, slot
-//              j = s*TPV + (l % TPV) of vertex l / TPV.
-//              idx plane  int4  (n0, n1, n2, -)    environment-local ids of
-//                                                  the tet's other vertices
-//              val planes Real4 (b_n0, p0) (b_n1, p1) (b_n2, p2)
+//              `steps` blocks of 32 slots, block s holds, for lane l, incident
+//              tet j = s*TPV + (l % TPV) of vertex l / TPV.  A slot is
+//              (n0, n1, n2, rid): the environment-local ids of the tet's
+//              other three vertices and the environment-local id of its
+//              record (ushort4 or int4, RecordFormat below); padding slots
+//              are zero.
+//   records    per environment, the distinct (b_n0, p0) (b_n1, p1) (b_n2, w)
+//              Real4 triples of its slots (EnvInfo::rbase, nrec):
 //              b_n = gradient of the tet's linear shape function of vertex n
 //              (a row of Dm^-1, or minus their sum), p0 = V*mu, p1 = V*lambda
-//              (material-adjusted), p2 = alpha (SNH) or 0.
+//              (material-adjusted), w = the slot's share of the tet's strain
+//              energy (1 / solved vertices of the tet).
 #pragma once
 #include <cstdint>
 
@@ -76,9 +80,9 @@ struct LoopControl {
   unsigned status;
 };
 
-// Slot record formats (both index a table of unique (b_n0, b_n1, b_n2, p)
-// records, 3 Real4 each, so slots that share a tet shape and material share
-// one table entry):
+// Slot formats (both index the environment's table of distinct records, 3
+// Real4 each, so slots that share a tet shape, material and energy weight
+// share one entry):
 //   kFmtIdx32  int4    (n0, n1, n2, record id)                     16 B/slot
 //   kFmtIdx16  ushort4 (n0, n1, n2, record id), all values < 65536  8 B/slot
 enum RecordFormat : int { kFmtIdx32 = 1, kFmtIdx16 = 2 };
