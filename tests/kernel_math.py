@@ -55,3 +55,25 @@ def slot_grad_hess(material, X4, x4, a, mu, lam):
     H = (p1 + p0) * np.outer(Fb, Fb) + p0 * (b @ b) * (F @ F.T) \
         + (p1 * trE * (b @ b) + 2 * p0 * (b @ E @ b)) * np.eye(3)
     return g, H
+
+
+def slot_energy(material, X4, x4, a, mu, lam):
+    """Strain energy of one tet seen from its vertex a, kernel closed form
+    (slot_energy in warpvbd_b200/csrc/vbd_device.cuh, before the slot weight):
+    SNH  p0/2 (Ic - 3 - ln(1 + (Ic - 3)/4)) + p1/2 (J - 1 - 3/4 p0/p1)^2, i.e.
+         the reference's mu'/2 (Ic - 3) - mu'/2 ln(Ic + 1) + lambda'/2 (J - alpha)^2
+         up to the constant mu'/2 ln 4, with J - 1 and Ic - 3 from G = F - I;
+    StVK p0 E:E + p1/2 tr(E)^2."""
+    b_all, vol = shape_gradients(X4)
+    p0, p1 = material_coeffs(material, mu, lam, vol)
+    u = x4 - X4
+    others = [q for q in range(4) if q != a]
+    G = sum(np.outer(u[n] - u[a], b_all[n]) for n in others)
+    t = np.trace(G)
+    if material == "snh":
+        Jm1 = t + 0.5 * (t * t - np.trace(G @ G)) + np.linalg.det(G)
+        Icm3 = 2.0 * t + np.sum(G * G)
+        r = Jm1 - 0.75 * p0 / p1
+        return 0.5 * p0 * (Icm3 - np.log1p(0.25 * Icm3)) + 0.5 * p1 * r * r
+    E = 0.5 * (G + G.T + G.T @ G)
+    return p0 * np.sum(E * E) + 0.5 * p1 * np.trace(E) ** 2

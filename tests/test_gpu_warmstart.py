@@ -245,3 +245,23 @@ def test_persistent_mode_trained_network_reduces_sweeps(n):
           f"{np.mean(it_w):.2f}; tip error vs converged FP64 plain {rel_p:.2e}, warm {rel_w:.2e}")
     assert np.mean(it_w[5:]) < np.mean(it_p[5:])
     assert rel_w < 5e-2
+
+
+def test_tiered_warm_start_is_bit_identical_to_one_launch():
+    """The warm-start stage decides per environment from its own potentials,
+    so the tiered launch (heavy environments on clusters, the rest in a
+    concurrent launch) must reproduce the single launch exactly."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(16, seed=6)
+    model = _trained()
+    one = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, cluster=4, block_threads=512)
+    two = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, cluster=4, block_threads=512,
+                           tiered=True)
+    one.set_warmstart(model)
+    two.set_warmstart(model)
+    for _ in range(10):
+        a = one.step(1e-3)
+        b = two.step(1e-3)
+        assert np.array_equal(a, b)
+        assert np.array_equal(one.env_status(), two.env_status())
+    assert np.array_equal(one.positions(), two.positions())
