@@ -155,6 +155,10 @@ int vbd_sync(vbd_solver* s);
 /* Sweep counts of the last step, n_env entries. */
 int vbd_get_iterations(vbd_solver* s, int* iterations_out);
 
+/* State in the caller's vertex order, float64 [n_vertices][3].  A host
+ * pointer to page-locked memory is copied directly (fastest).  Setting the
+ * positions keeps the learned warm start's history (valid when the caller
+ * hands back what a step produced); vbd_reset clears it. */
 int vbd_get_positions(vbd_solver* s, double* positions_out);
 int vbd_set_positions(vbd_solver* s, const double* positions);
 int vbd_get_velocities(vbd_solver* s, double* velocities_out);
@@ -176,6 +180,10 @@ typedef struct vbd_info_t {
   int cluster;          /* block mode: thread blocks per cluster */
   int n_blocks;         /* block mode: blocks of the current work map (> n_env: some
                            environments are split over a cluster) */
+  int last_step_launches;     /* kernels the last finished step launched */
+  float last_step_kernel_ms;  /* CUDA-event time of its step kernels (the sweeps: block,
+                                 persistent or graph launch, both tiers), without the
+                                 warm-start feature and inference kernels */
 } vbd_info_t;
 int vbd_get_info(vbd_solver* s, vbd_info_t* info);
 

@@ -59,7 +59,8 @@ class VBDInfo(ctypes.Structure):
         "block_threads", "precision", "material")] + [
         ("n_slots", ctypes.c_longlong), ("n_slot_records", ctypes.c_longlong),
         ("device_bytes", ctypes.c_longlong), ("n_unique_records", ctypes.c_int),
-        ("record_format", ctypes.c_int), ("cluster", ctypes.c_int), ("n_blocks", ctypes.c_int)]
+        ("record_format", ctypes.c_int), ("cluster", ctypes.c_int), ("n_blocks", ctypes.c_int),
+        ("last_step_launches", ctypes.c_int), ("last_step_kernel_ms", ctypes.c_float)]
 
 
 # every entry point declared in include/vbd_b200.h: name -> (restype, argtypes)

@@ -492,6 +492,11 @@ struct vbd_solver {
   DevBuf<int4> d_work2;
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // timing of the step kernels of every step (events around them on the
+  // solver's stream) and the number of kernels the step launched
+  cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;
+  int launches_pending = 0, launches_last = 0;
+  float kernel_ms_last = 0.f;
   // learned warm start
   DevBuf<float4> d_wstat;
   DevBuf<int2> d_chunk_owner;
@@ -573,6 +578,8 @@ void free_solver(vbd_solver* s) {
   s->d_work.release();
   s->d_work2.release();
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_k0) cudaEventDestroy(s->ev_k0);
+  if (s->ev_k1) cudaEventDestroy(s->ev_k1);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
   if (s->aux) {
     cudaStreamSynchronize(s->aux);
@@ -873,6 +880,8 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   };
   int err = 0;
   if (bad(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream")) err = 1;
+  if (!err && (bad(cudaEventCreate(&s->ev_k0), "event") || bad(cudaEventCreate(&s->ev_k1), "event")))
+    err = 1;
   cudaStream_t st = s->stream;
   const Layout& L = s->L;
   if (!err && bad(s->d_env.upload(L.env, st), "env")) err = 1;
@@ -1134,6 +1143,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
   if (rc != VBD_OK) return rc;
   const DevMesh m = s->mesh();
   cudaStream_t st = s->stream;
+  int launches = 0;
   if (s->mode == VBD_MODE_BLOCK) {
     const double* dtol = nullptr;
     if (tol_env) {
@@ -1148,14 +1158,18 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
                                   s->ws_history ? 1 : 0, s->d_wpack.p, s->d_feat.p, st));
       CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
                                s->d_pred.p, s->d_ws_err.p, st));
+      launches += 3;  // pack, features, inference
     }
+    CUDA_TRY(cudaEventRecord(s->ev_k0, st));
     if (!s->tiered) {
+      ++launches;
       CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
                                s->d_work.p, (int)s->work.size(), s->cluster, s->smem_bytes, st));
     } else {
       // heavy launch first (its clusters need whole groups of free SMs), the
       // light launch beside it on the second stream, joined before the end
       const bool two = !s->work.empty() && !s->work2.empty();
+      launches += (s->work.empty() ? 0 : 1) + (s->work2.empty() ? 0 : 1);
       if (two) CUDA_TRY(cudaEventRecord(s->ev_fork, st));
       if (!s->work.empty())
         CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->heavy_threads, m,
@@ -1179,15 +1193,22 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
                                   s->ws_history ? 1 : 0, s->d_wpack.p, s->d_feat.p, st));
       CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
                                s->d_pred.p, s->d_ws_err.p, st));
+      launches += 3;
     }
+    CUDA_TRY(cudaEventRecord(s->ev_k0, st));
+    ++launches;
     CUDA_TRY(launch_persist(s->prec, s->material, s->tpv, s->threads, m, s->d_params.p,
                             s->d_pctl.p, s->persist_blocks, s->wait_limits, s->d_pparts.p,
                             s->persist_smem, st));
   } else if (s->mode == VBD_MODE_GRAPH) {
     rc = build_graph(s);
     if (rc != VBD_OK) return rc;
+    CUDA_TRY(cudaEventRecord(s->ev_k0, st));
     CUDA_TRY(cudaGraphLaunch(s->graph_exec, st));
+    launches = -1;  // begin + sweeps x (colours + check) + end: counted in finish
   } else {
+    CUDA_TRY(cudaEventRecord(s->ev_k0, st));
+    launches = -1;
     // host-driven loop: one device->host read of the loop state per sweep
     CUDA_TRY(launch_begin(s->state64, m, s->d_params.p, s->d_ctl.p, st));
     const EnvInfo& e = s->L.env[0];
@@ -1205,6 +1226,8 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
     }
     CUDA_TRY(launch_end(s->state64, m, s->d_params.p, s->d_ctl.p, st));
   }
+  CUDA_TRY(cudaEventRecord(s->ev_k1, st));
+  s->launches_pending = launches;
   s->pending = true;
   s->ws_history = true;  // ut now holds this step's inertia target
   return VBD_OK;
@@ -1232,6 +1255,13 @@ int finish(vbd_solver* s, int* iters_out) {
                              cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   s->pending = false;
+  if (cudaEventElapsedTime(&s->kernel_ms_last, s->ev_k0, s->ev_k1) != cudaSuccess) {
+    s->kernel_ms_last = -1.f;
+    cudaGetLastError();  // not a step failure: keep it out of the next launch check
+  }
+  s->launches_last = s->launches_pending >= 0
+                         ? s->launches_pending
+                         : 2 + s->h_iters[0] * ((int)s->L.color.size() + 1);
   if (iters_out) std::memcpy(iters_out, s->h_iters, sizeof(int) * s->n_env);
   s->last_status = status_from_bits(s, s->h_status);
   if (s->last_status >= 0) {
@@ -1401,7 +1431,11 @@ static int exchange(vbd_solver* s, const double* in, double* out, bool positions
   const size_t bytes = sizeof(double) * 3 * (size_t)s->V;
   void* state = positions ? (void*)s->d_u.p : (void*)s->d_vel.p;
   const double* off = positions ? s->d_X.p : nullptr;
-  if (in) s->ws_history = false;  // a new state: no previous inertia target
+  // The warm start's history feature (u minus the previous step's inertia
+  // target) is kept: a caller handing back the positions a step produced
+  // (the usual loop) keeps it valid, and after an unrelated state it only
+  // makes the prediction worse, which the potential check then rejects.
+  // vbd_reset clears it.
   if (out) {
     CUDA_TRY(launch_gather(s->state64, off, s->d_map.p, state, s->d_io.p, s->V, st));
     CUDA_TRY(cudaMemcpyAsync(out, s->d_io.p, bytes, cudaMemcpyDeviceToHost, st));
@@ -1447,6 +1481,8 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
   info->n_unique_records = s->L.table.size();
   info->record_format = s->fmt == kFmtIdx16 ? 8 : 16;
   info->cluster = s->cluster;
+  info->last_step_launches = s->launches_last;
+  info->last_step_kernel_ms = s->kernel_ms_last;
   info->n_blocks = s->mode == VBD_MODE_PERSIST ? s->persist_blocks
                                                 : (int)(s->work.size() + s->work2.size());
   return VBD_OK;
