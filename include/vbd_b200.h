@@ -137,6 +137,19 @@ void vbd_destroy(vbd_solver* s);
  * vbd_reset / vbd_set_positions).  Defaults: 2^26 polls, 2 s. */
 int vbd_set_wait_limits(vbd_solver* s, long long max_polls, unsigned long long max_wait_ns);
 
+/* No counterpart in the reference.  Step timeline of the block mode: after
+ * vbd_set_trace(s, 1) every step records, per thread block of its
+ * environment launches, four words:
+ *   [0] global timer at the block's start (ns)   [1] at its end (ns)
+ *   [2] (environment << 32) | (rank in its cluster << 16) | SM id
+ *   [3] (sweeps << 8) | launch (0: the single or heavy launch, 1: light)
+ * (blocks without an environment, padding a cluster, leave zeros).
+ * vbd_get_trace copies the last finished step's records, at most `cap`, and
+ * writes their number to *count (records = NULL: only the number); the other
+ * modes record nothing (count 0). */
+int vbd_set_trace(vbd_solver* s, int enable);
+int vbd_get_trace(vbd_solver* s, unsigned long long* records, int cap, int* count);
+
 /* VBDSolver.reset (vbd_solver.py:501-506): positions back to rest, velocity 0 */
 int vbd_reset(vbd_solver* s);
 
@@ -210,6 +223,9 @@ int vbd_set_warmstart(vbd_solver* s, const float* params, const float* norm);
 /* Features of the coming step of length dt at the current state, into device
  * [n_vertices][feature_width]. */
 int vbd_ws_features(vbd_solver* s, double dt, float* features);
+/* Row of every caller vertex in the feature, target and prediction arrays:
+ * host int32 [n_vertices]. */
+int vbd_ws_vertex_rows(vbd_solver* s, int32_t* rows);
 /* After a step: the correction it converged to, (x_new - inertia guess) / h,
  * into device [n_vertices][3] (zero rows where features flag 0). */
 int vbd_ws_targets(vbd_solver* s, const float* features, float* targets);

@@ -64,3 +64,73 @@ def loss_and_grad(p, X, Y):
     g["W1"] = d1.T @ x
     g["b1"] = d1.sum(0)
     return loss, pack(g), float((d * d).sum())
+
+
+def vertex_constants(X, tets, E, nu, rho):
+    """Per-vertex warm-start constants (h, log10(E/(rho h^2)), nu, valence/20)
+    and the valence, from incident-tet means: h is the mean of cbrt(6 V_t),
+    log E, rho and nu are plain means over the incident tets."""
+    X = np.asarray(X, np.float64)
+    T = np.asarray(tets, np.int64).reshape(-1, 4)
+    n = X.shape[0]
+    D = np.stack([X[T[:, i]] - X[T[:, 3]] for i in range(3)], axis=2)
+    vol = np.abs(np.linalg.det(D)) / 6.0
+    k = np.bincount(T.reshape(-1), minlength=n).astype(np.float64)
+
+    def vmean(per_tet):
+        s = np.zeros(n)
+        for i in range(4):
+            np.add.at(s, T[:, i], per_tet)
+        return np.divide(s, k, out=np.zeros(n), where=k > 0)
+    h = vmean(np.cbrt(6.0 * vol))
+    logE, r, v = vmean(np.log10(E)), vmean(rho), vmean(nu)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        w1 = np.where(k > 0, logE - np.log10(r * h * h), 0.0)
+    return np.stack([np.where(k > 0, h, 1.0), w1, v, k / 20.0], 1), k.astype(np.int64)
+
+
+def features(X, tets, E, nu, rho, active, x, v, dt, g, x_prev=None, v_prev=None):
+    """Feature rows [n, 24] of the coming step of length dt at state (x, v)
+    (positions, velocities); x_prev, v_prev: the state the previous step
+    started from (None before the first step: no history).  Rows of vertices
+    that are not solved (fixed or without tets) are zero.  Row layout:
+    0-2 inertia displacement v dt + g dt^2, 3-5 v dt, 6-8 1-ring mean of the
+    neighbours' v dt minus the vertex's own, 9-11 the same for the
+    displacement from rest, 12-14 the previous step's correction
+    x - (x_prev + v_prev dt + g dt^2), 15-17 g dt^2 -- all divided by h and
+    then by s, the RMS of the 18 -- then log10(E dt^2/(rho h^2)), nu,
+    valence/20, log10 s, s, 1.  Neighbours count once per incident tet."""
+    X = np.asarray(X, np.float64)
+    T = np.asarray(tets, np.int64).reshape(-1, 4)
+    n = X.shape[0]
+    ws, k = vertex_constants(X, T, E, nu, rho)
+    u = np.asarray(x, np.float64) - X
+    vel = np.asarray(v, np.float64)
+    g2 = np.asarray(g, np.float64) * dt * dt
+    su, sv = np.zeros((n, 3)), np.zeros((n, 3))
+    for a in range(4):
+        for b in range(4):
+            if a != b:
+                np.add.at(su, T[:, a], u[T[:, b]] - u[T[:, a]])
+                np.add.at(sv, T[:, a], vel[T[:, b]] - vel[T[:, a]])
+    solved = np.asarray(active, bool) & (k > 0)
+    cnt = np.maximum(3 * k, 1)[:, None]
+    ih = 1.0 / ws[:, :1]
+    if x_prev is not None:
+        target = np.asarray(x_prev, np.float64) - X + np.asarray(v_prev, np.float64) * dt + g2
+        up = u - target
+    else:
+        up = np.zeros((n, 3))
+    d = np.concatenate([(vel * dt + g2) * ih, vel * dt * ih, sv / cnt * dt * ih, su / cnt * ih,
+                        up * ih, np.broadcast_to(g2, (n, 3)) * ih], 1)
+    s = np.sqrt((d * d).mean(1)) + 1e-30
+    out = np.zeros((n, 24))
+    out[:, :18] = d / s[:, None]
+    out[:, 18] = ws[:, 1] + 2.0 * np.log10(dt)
+    out[:, 19] = ws[:, 2]
+    out[:, 20] = ws[:, 3]
+    out[:, 21] = np.log10(s)
+    out[:, 22] = s
+    out[:, 23] = 1.0
+    out[~solved] = 0.0
+    return out

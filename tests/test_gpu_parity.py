@@ -224,6 +224,34 @@ def test_tiered_launch_is_bit_identical_to_one_launch(cluster, threads):
     assert np.array_equal(one.velocities(), two.velocities())
 
 
+def test_step_timeline():
+    """The traced tiered step computes the same as the untraced one, and its
+    timeline holds every block once: each environment with its sweep count,
+    split environments on `cluster` blocks of the heavy launch."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(24, seed=4)
+    kw = dict(dx_tol=1e-7, max_iter=1000, cluster=4, block_threads=256, tiered=True)
+    ref, traced = BatchedVBDSolver(envs, **kw), BatchedVBDSolver(envs, **kw)
+    traced.set_trace(True)
+    for _ in range(4):
+        a = ref.step(1e-3)
+        b = traced.step(1e-3)
+        assert np.array_equal(a, b)
+        tl = traced.timeline()
+        assert np.all(tl["end_ns"] >= tl["start_ns"]) and tl["start_ns"].min() == 0
+        assert sorted(set(tl["env"].tolist())) == list(range(len(envs)))
+        for e in range(len(envs)):
+            rows = tl["env"] == e
+            assert np.all(tl["sweeps"][rows] == b[e])
+            n = int(rows.sum())
+            assert (n, set(tl["launch"][rows].tolist())) in ((1, {1}), (4, {0}))
+            assert sorted(tl["rank"][rows].tolist()) == list(range(n))
+    assert np.array_equal(ref.positions(), traced.positions())
+    traced.set_trace(False)
+    traced.step(1e-3)
+    assert len(traced.timeline()["env"]) == 0
+
+
 def test_downloads_into_caller_arrays():
     """positions(out=...) / DeviceArray.numpy(out=...) fill a caller array
     (e.g. page-locked) with exactly what a fresh download returns."""

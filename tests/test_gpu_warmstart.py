@@ -102,6 +102,41 @@ def test_features_and_targets():
     assert np.abs(f2[solved, 12:15]).max() > 0   # history after a step
 
 
+@pytest.mark.parametrize("tpv", [2, 4, 16])
+def test_features_match_oracle(tpv):
+    """Feature rows of the kernel (fp32 sums and arithmetic on fp64 state)
+    against the FP64 numpy restatement, before the first step (no history)
+    and after four steps (with the previous step's correction)."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(3, seed=11)
+    sol = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, tpv=tpv)
+    X = np.concatenate([e.vertices for e in envs])
+    off = np.cumsum([0] + [e.n_vertices for e in envs])
+    T = np.concatenate([e.tets + o for e, o in zip(envs, off)])
+    E, nu, rho = (np.concatenate([getattr(e, a) for e in envs])
+                  for a in ("youngs", "poisson", "density"))
+    act = np.concatenate([e.active for e in envs])
+    rows = sol.ws_vertex_rows()
+    assert sorted(rows.tolist()) == list(range(len(X)))
+    dt, g = 1e-3, (0.0, 0.0, -9.81)
+
+    def check(expect):
+        got = sol.ws_features(dt).cpu().numpy().astype(np.float64)[rows]
+        solved = expect[:, 23] > 0
+        assert np.array_equal(got[:, 23] > 0, solved)
+        # scale-free columns: absolute; s (column 22): relative
+        err = np.abs(got[solved][:, :22] - expect[solved][:, :22])
+        rel = np.abs(got[solved, 22] / expect[solved, 22] - 1)
+        print(f"tpv {tpv}: feature error {err.max():.2e}, scale {rel.max():.2e}")
+        assert err.max() < 2e-5 and rel.max() < 1e-5
+
+    check(mo.features(X, T, E, nu, rho, act, X, np.zeros_like(X), dt, g))
+    for _ in range(4):
+        x0, v0 = sol.positions(), sol.velocities()
+        sol.step(dt)
+    check(mo.features(X, T, E, nu, rho, act, sol.positions(), sol.velocities(), dt, g, x0, v0))
+
+
 def test_rejected_prediction_reproduces_plain_vbd_exactly():
     """A network with huge random weights raises the incremental potential;
     every environment must fall back to the inertia guess, which makes the

@@ -37,3 +37,27 @@ def test_fold_normalization_is_exact():
     raw = ws.fold_normalization(p, mu_x, sd_x, mu_y, sd_y)
     out_raw, _ = mo.forward(raw.astype(np.float64), X)
     assert np.allclose(out_raw, out_n * sd_y + mu_y, rtol=1e-5, atol=1e-5)
+
+
+def test_feature_oracle_invariants():
+    """The feature restatement: zero rows for fixed vertices, unit RMS of the
+    18 displacement-type entries, invariance of the 1-ring columns under a
+    rigid translation, and the rest-state row (only gravity terms)."""
+    from warpvbd_b200 import scenes
+    s = scenes.cantilever(10, 2, 2)
+    X, T = s.vertices, s.tets
+    rng = np.random.default_rng(0)
+    x = X + 1e-3 * rng.normal(size=X.shape)
+    v = 0.1 * rng.normal(size=X.shape)
+    f = mo.features(X, T, s.youngs, s.poisson, s.density, s.active, x, v, 1e-3, (0, 0, -9.81))
+    solved = f[:, 23] > 0
+    assert np.array_equal(solved, s.active)
+    assert np.all(f[~solved] == 0)
+    assert np.allclose(np.sqrt((f[solved, :18] ** 2).mean(1)), 1.0)
+    f2 = mo.features(X, T, s.youngs, s.poisson, s.density, s.active, x + 0.3, v, 1e-3,
+                     (0, 0, -9.81))
+    assert np.allclose(f2, f, atol=1e-9)
+    r = mo.features(X, T, s.youngs, s.poisson, s.density, s.active, X, 0 * X, 1e-3,
+                    (0, 0, -9.81))[solved]
+    assert np.allclose(r[:, 0:3], r[:, 15:18]) and np.all(r[:, 3:15] == 0)
+    assert np.allclose(r[:, 20] * 20, np.bincount(T.reshape(-1), minlength=len(X))[solved])

@@ -80,6 +80,10 @@ SIGNATURES = {
     "vbd_destroy": (None, [_vp]),
     "vbd_reset": (ctypes.c_int, [_vp]),
     "vbd_set_wait_limits": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_ulonglong]),
+    "vbd_set_trace": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "vbd_get_trace": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int,
+                                     _ip]),
+    "vbd_ws_vertex_rows": (ctypes.c_int, [_vp, _i]),
     "vbd_step": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip]),
     "vbd_step_batched": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _d,
                                         ctypes.c_int, _ip]),

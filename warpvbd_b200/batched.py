@@ -98,6 +98,35 @@ class BatchedVBDSolver:
     def stream(self):
         return _lib.load().vbd_get_stream(self._h)
 
+    def set_trace(self, enable=True):
+        """Record a timeline of every later step (block mode): per thread
+        block of the environment launches, its start and end on the GPU's
+        global timer; see ``timeline``."""
+        _lib.check(_lib.load().vbd_set_trace(self._h, 1 if enable else 0), "vbd_set_trace")
+
+    def timeline(self):
+        """Timeline of the last finished traced step, one row per thread
+        block: dict of arrays start_ns, end_ns (relative to the earliest
+        start), env, rank (in its cluster), sm, sweeps, launch (0 the single
+        or heavy launch, 1 the light launch of a tiered step)."""
+        L = _lib.load()
+        n = ctypes.c_int(0)
+        _lib.check(L.vbd_get_trace(self._h, None, 0, ctypes.byref(n)), "vbd_get_trace")
+        cap = n.value
+        rec = np.zeros((max(cap, 1), 4), np.uint64)
+        _lib.check(L.vbd_get_trace(self._h, rec.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)),
+                                   cap, ctypes.byref(n)), "vbd_get_trace")
+        rec = rec[:n.value]
+        rec = rec[rec[:, 0] > 0]  # padding blocks of a cluster record nothing
+        t0 = rec[:, 0].min() if len(rec) else np.uint64(0)
+        return {"start_ns": (rec[:, 0] - t0).astype(np.int64),
+                "end_ns": (rec[:, 1] - t0).astype(np.int64),
+                "env": (rec[:, 2] >> np.uint64(32)).astype(np.int64),
+                "rank": ((rec[:, 2] >> np.uint64(16)) & np.uint64(0xFFFF)).astype(np.int64),
+                "sm": (rec[:, 2] & np.uint64(0xFFFF)).astype(np.int64),
+                "sweeps": (rec[:, 3] >> np.uint64(8)).astype(np.int64),
+                "launch": (rec[:, 3] & np.uint64(0xFF)).astype(np.int64)}
+
     def step(self, dt=1e-3, dx_tol=None, tol_per_env=None, max_iter=None, blocking=True):
         """Step every environment; returns the per-environment sweep counts
         (blocking) or None (enqueued only; see ``sync``)."""
@@ -163,6 +192,14 @@ class BatchedVBDSolver:
 
     def ws_features(self, dt, out=None):
         return _ws_features(self._h, self.n_vertices, dt, out)
+
+    def ws_vertex_rows(self):
+        """Row of every vertex (caller order) in the feature, target and
+        prediction arrays."""
+        rows = np.zeros(self.n_vertices, np.int32)
+        _lib.check(_lib.load().vbd_ws_vertex_rows(self._h, _lib.ptr(rows, "i")),
+                   "vbd_ws_vertex_rows")
+        return rows
 
     def ws_targets(self, features, out=None):
         return _ws_targets(self._h, self.n_vertices, features, out)

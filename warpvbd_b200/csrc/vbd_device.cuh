@@ -23,6 +23,17 @@ template <typename Real>
 using real4 = typename V4<Real>::type;
 
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned sm_id() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return r;
+}
 __device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
 __device__ __forceinline__ double4 ldcg4(const double4* p) {
   const double2* q = reinterpret_cast<const double2*>(p);

@@ -497,6 +497,11 @@ struct vbd_solver {
   cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;
   int launches_pending = 0, launches_last = 0;
   float kernel_ms_last = 0.f;
+  // block-mode timeline (vbd_set_trace): 4 words per block of the step's
+  // launches, heavy / single launch first, then the light launch
+  bool trace_on = false;
+  DevBuf<unsigned long long> d_trace;
+  int trace_pending = 0, trace_last = 0;
   // learned warm start
   DevBuf<float4> d_wstat;
   DevBuf<int2> d_chunk_owner;
@@ -577,6 +582,7 @@ void free_solver(vbd_solver* s) {
   s->d_tol.release();
   s->d_work.release();
   s->d_work2.release();
+  s->d_trace.release();
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_k0) cudaEventDestroy(s->ev_k0);
   if (s->ev_k1) cudaEventDestroy(s->ev_k1);
@@ -684,7 +690,7 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
     for (int r = 0; r < C; ++r) work.push_back(make_int4(order[i], r, C, 0));
   if (s->tiered) {
     // the others run one block each in the light launch
-    for (int i = best_h; i < n; ++i) work2.push_back(make_int4(order[i], 0, 1, 0));
+    for (int i = best_h; i < n; ++i) work2.push_back(make_int4(order[i], 0, 1, 1));
     return;
   }
   int in_cluster = 0;
@@ -1075,6 +1081,7 @@ int set_params(vbd_solver* s, double dt, double tol, int max_iter) {
   p.strict_spd = (s->flags & VBD_STRICT_SPD) ? 1 : 0;
   p.warm = s->warm ? 1 : 0;
   p.tab_in_smem = s->tab_in_smem ? 1 : 0;
+  p.trace = (s->trace_on && s->mode == VBD_MODE_BLOCK) ? s->d_trace.p : nullptr;
   if (s->params_valid && std::memcmp(&p, &s->cur_params, sizeof p) == 0) return VBD_OK;
   // the pinned staging struct may still be read by an earlier copy
   CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -1152,6 +1159,8 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
                           cudaMemcpyHostToDevice));
       dtol = s->d_tol.p;
     }
+    if (s->cur_params.trace)
+      CUDA_TRY(cudaMemsetAsync(s->d_trace.p, 0, sizeof(unsigned long long) * s->d_trace.n, st));
     if (s->warm) {
       // features of the coming step, then the network's predicted corrections
       CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
@@ -1178,9 +1187,10 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
       if (!s->work2.empty()) {
         cudaStream_t ls = two ? s->aux : st;
         if (two) CUDA_TRY(cudaStreamWaitEvent(ls, s->ev_fork, 0));
-        CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params,
-                                 dtol, s->d_work2.p, (int)s->work2.size(), 1, s->smem_light,
-                                 ls));
+        StepParams lp = s->cur_params;
+        if (lp.trace) lp.trace += 4 * s->work.size();
+        CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, lp, dtol,
+                                 s->d_work2.p, (int)s->work2.size(), 1, s->smem_light, ls));
         if (two) {
           CUDA_TRY(cudaEventRecord(s->ev_join, ls));
           CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
@@ -1228,6 +1238,9 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
   }
   CUDA_TRY(cudaEventRecord(s->ev_k1, st));
   s->launches_pending = launches;
+  s->trace_pending = s->cur_params.trace && s->mode == VBD_MODE_BLOCK
+                         ? (int)(s->work.size() + s->work2.size())
+                         : 0;
   s->pending = true;
   s->ws_history = true;  // ut now holds this step's inertia target
   return VBD_OK;
@@ -1259,6 +1272,7 @@ int finish(vbd_solver* s, int* iters_out) {
     s->kernel_ms_last = -1.f;
     cudaGetLastError();  // not a step failure: keep it out of the next launch check
   }
+  s->trace_last = s->trace_pending;
   s->launches_last = s->launches_pending >= 0
                          ? s->launches_pending
                          : 2 + s->h_iters[0] * ((int)s->L.color.size() + 1);
@@ -1368,6 +1382,37 @@ int vbd_set_wait_limits(vbd_solver* s, long long max_polls, unsigned long long m
   if (max_polls < 0) return fail(VBD_ERR_INVALID_ARG, "max_polls must be >= 0");
   s->wait_limits.max_polls = max_polls;
   s->wait_limits.max_wait_ns = max_wait_ns;
+  return VBD_OK;
+}
+
+int vbd_set_trace(vbd_solver* s, int enable) {
+  if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  DeviceGuard dg(s->device);
+  if (enable && !s->d_trace.p) {
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    CUDA_TRY(s->d_trace.alloc(4 * (s->d_work.n + s->d_work2.n)));
+    CUDA_TRY(cudaMemset(s->d_trace.p, 0, sizeof(unsigned long long) * s->d_trace.n));
+  }
+  s->trace_on = enable != 0;
+  return VBD_OK;
+}
+
+int vbd_get_trace(vbd_solver* s, unsigned long long* records, int cap, int* count) {
+  if (!s || !count) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  DeviceGuard dg(s->device);
+  if (s->pending) {
+    const int rc = finish(s, nullptr);
+    if (rc < 0) return rc;
+  }
+  if (!records) {
+    *count = s->trace_last;
+    return VBD_OK;
+  }
+  const int n = std::min(std::max(cap, 0), s->trace_last);
+  if (n > 0)
+    CUDA_TRY(cudaMemcpy(records, s->d_trace.p, sizeof(unsigned long long) * 4 * (size_t)n,
+                        cudaMemcpyDeviceToHost));
+  *count = n;
   return VBD_OK;
 }
 
@@ -1551,6 +1596,12 @@ int vbd_ws_features(vbd_solver* s, double dt, float* features) {
   CUDA_TRY(launch_ws_features(s->prec, s->tpv, s->mesh(), (int)s->L.chunk.size(), dt, s->g,
                               s->ws_history ? 1 : 0, s->d_wpack.p, features, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return VBD_OK;
+}
+
+int vbd_ws_vertex_rows(vbd_solver* s, int32_t* rows) {
+  if (!s || !rows) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  std::memcpy(rows, s->L.new_of_old.data(), sizeof(int32_t) * (size_t)s->V);
   return VBD_OK;
 }
 

@@ -69,6 +69,7 @@ struct StepParams {
   int strict_spd;
   int warm;  // start from the learned prediction (DevMesh::ws_pred) when it lowers the energy
   int tab_in_smem;  // block mode: the launch's shared memory holds each environment's records
+  unsigned long long* trace;  // block mode: 4 words per block of the launch, or null
 };
 
 // Grid-mode loop control (one per solver).

@@ -309,6 +309,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
   const int4 w = work[blockIdx.x];
   const int env = w.x, rank = w.y, g = w.z;
   if (env < 0) return;  // padding block of a cluster of single-block environments
+  const unsigned long long t_start = p.trace ? globaltimer_ns() : 0ull;
   const EnvInfo e = m.env[env];
   const StepConst sc = make_const(p);
   // the environment's record table: staged in shared memory after the state
@@ -373,6 +374,13 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
   if (threadIdx.x == 0 && rank == 0) {
     m.iters[env] = it;
     m.status[env] = s_stat | (converged ? 0u : kStatIterCap);
+  }
+  if (p.trace && threadIdx.x == 0) {
+    unsigned long long* r = p.trace + 4 * (size_t)blockIdx.x;
+    r[0] = t_start;
+    r[1] = globaltimer_ns();
+    r[2] = ((unsigned long long)env << 32) | ((unsigned long long)rank << 16) | sm_id();
+    r[3] = ((unsigned long long)it << 8) | (unsigned long long)w.w;
   }
 }
 

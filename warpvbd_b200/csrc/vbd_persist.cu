@@ -62,11 +62,6 @@ struct CoherentState {
   __device__ __forceinline__ void store(int i, const real4<SReal>& v) const { p[i] = v; }
 };
 
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
   unsigned long long v;

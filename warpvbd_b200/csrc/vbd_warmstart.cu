@@ -64,9 +64,10 @@ __global__ void ws_pack_kernel(DevMesh m, float4* __restrict__ pa, float2* __res
 }
 
 template <typename SReal, int TPV, int FMT>
-__global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunks, double dt,
-                                                          double gx, double gy, double gz,
-                                                          int history, const float4* __restrict__ pa,
+__global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunks, float dt,
+                                                          float gx, float gy, float gz,
+                                                          float log_dt2, int history,
+                                                          const float4* __restrict__ pa,
                                                           const float2* __restrict__ pb,
                                                           float* __restrict__ feat) {
   using S4 = real4<SReal>;
@@ -121,34 +122,46 @@ __global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunk
       sv[i] += __shfl_xor_sync(0xffffffffu, sv[i], off);
     }
   }
-  if (!valid || sub != 0) return;
+  if (!valid) return;
+  // every lane of the vertex holds the sums now; each computes the row and
+  // stores its share of the six 16-byte pieces
   const float4 ws = m.wstat[gv];
-  const double h = ws.x, ih = 1.0 / h;
-  const double cnt = 3.0 * k;
+  const float ih = 1.0f / ws.x;
+  const float icnt = 1.0f / float(3 * k);
   const S4 tp = reinterpret_cast<const S4*>(m.ut)[gv];  // the previous step's inertia target
-  float* f = feat + (size_t)gv * kWsRow;
-  const double g2[3] = {gx * dt * dt, gy * dt * dt, gz * dt * dt};
-  const double v[3] = {double(vo.x), double(vo.y), double(vo.z)};
-  const double up[3] = {double(uo.x - tp.x), double(uo.y - tp.y), double(uo.z - tp.z)};
-  double d[18];
+  const float dt2 = dt * dt;
+  const float g2[3] = {gx * dt2, gy * dt2, gz * dt2};
+  const float v[3] = {vx, vy, vz};
+  // the correction u - ut_prev is a difference of nearby values: take it in
+  // the state precision before rounding
+  const float up[3] = {float(uo.x - tp.x), float(uo.y - tp.y), float(uo.z - tp.z)};
+  float r[kWsRow];
+#pragma unroll
   for (int i = 0; i < 3; ++i) {
-    d[i] = (v[i] * dt + g2[i]) * ih;
-    d[3 + i] = v[i] * dt * ih;
-    d[6 + i] = sv[i] / cnt * dt * ih;
-    d[9 + i] = su[i] / cnt * ih;
-    d[12 + i] = history ? up[i] * ih : 0.0;
-    d[15 + i] = g2[i] * ih;
+    r[i] = (v[i] * dt + g2[i]) * ih;
+    r[3 + i] = v[i] * dt * ih;
+    r[6 + i] = sv[i] * icnt * dt * ih;
+    r[9 + i] = su[i] * icnt * ih;
+    r[12 + i] = history ? up[i] * ih : 0.0f;
+    r[15 + i] = g2[i] * ih;
   }
-  double ss = 0.0;
-  for (int i = 0; i < 18; ++i) ss += d[i] * d[i];
-  const double sc = sqrt(ss / 18.0) + 1e-30;
-  for (int i = 0; i < 18; ++i) f[i] = float(d[i] / sc);
-  f[18] = ws.y + float(2.0 * log10(dt));
-  f[19] = ws.z;
-  f[20] = ws.w;
-  f[21] = float(log10(sc));
-  f[22] = float(sc);
-  f[23] = 1.0f;
+  float ss = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 18; ++i) ss += r[i] * r[i];
+  const float sc = sqrtf(ss * (1.0f / 18.0f)) + 1e-30f;
+  const float isc = 1.0f / sc;
+#pragma unroll
+  for (int i = 0; i < 18; ++i) r[i] *= isc;
+  r[18] = ws.y + log_dt2;
+  r[19] = ws.z;
+  r[20] = ws.w;
+  r[21] = log10f(sc);
+  r[22] = sc;
+  r[23] = 1.0f;
+  float4* f = reinterpret_cast<float4*>(feat + (size_t)gv * kWsRow);
+#pragma unroll
+  for (int j = 0; j < kWsRow / 4; ++j)
+    if (j % TPV == sub) f[j] = make_float4(r[4 * j], r[4 * j + 1], r[4 * j + 2], r[4 * j + 3]);
 }
 
 // Training target after a step: (u - ut) / (h s) for solved vertices.
@@ -322,8 +335,9 @@ struct FeatLaunch {
     float4* pa = reinterpret_cast<float4*>(pack);
     float2* pb = reinterpret_cast<float2*>(pack + 4 * (size_t)m.n_vertices);
     ws_pack_kernel<SReal><<<(m.n_vertices + 255) / 256, 256, 0, s>>>(m, pa, pb);
-    ws_features_kernel<SReal, TPV, FMT><<<blocks, 256, 0, s>>>(m, n_chunks, dt, gx, gy, gz,
-                                                               history, pa, pb, feat);
+    ws_features_kernel<SReal, TPV, FMT><<<blocks, 256, 0, s>>>(
+        m, n_chunks, float(dt), float(gx), float(gy), float(gz), float(2.0 * log10(dt)), history,
+        pa, pb, feat);
     return cudaGetLastError();
   }
 };
