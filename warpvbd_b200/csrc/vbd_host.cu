@@ -634,25 +634,38 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
   return with_tab ? state + (size_t)ei.nrec * s->rec_bytes : state;
 }
 
-// Block-mode work map.  Each environment's work estimate is its slot count
-// times its last sweep count (1 before the first step).  With cluster > 1 the
-// heaviest environments may each take a whole cluster (group = cluster); the
-// others take one block each, packed `cluster` to a cluster, heaviest first.
-// The split set is the one with the smallest predicted step time: the
-// largest of (heaviest single-block environment, heaviest split environment
-// / (cluster * efficiency), total work / resident blocks).
+// Block-mode work map.  Each environment's duration is predicted from its
+// slot count and its expected sweep count (a slowly decaying maximum of its
+// past counts; 1 before the first step) with a per-sweep cost model measured
+// on B200 at 512 threads, in units of one slot visit of a single block:
+//   one block              sweeps * (slots + 8300)
+//   split over C blocks    sweeps * (slots / C + I_C),
+//                          I_C = 10300 / 11200 / 12200 / 16500 for C = 2 / 4 / 8 / 16
+// (the fixed part is the per-colour barrier and dependency chain: a
+// 7K-slot environment costs 29 us per sweep, a 44K-slot one 110 us; a
+// 68K-slot environment 129 / 77 / 49 / 36 / 36 us on 1 / 2 / 4 / 8 / 16
+// blocks).  With cluster > 1 the longest environments may each take a whole
+// cluster (group = cluster); the split set is the one with the smallest
+// predicted step time, the largest of (longest split environment, longest
+// single-block environment, all block time / resident blocks).  Blocks are
+// listed longest first, which the block scheduler then starts first.
 void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
                std::vector<int4>& work2) {
   const int n = s->n_env, C = s->cluster;
   work2.clear();
-  std::vector<double> w(n);
+  const double a1 = 8300.0;
+  const double aC = C == 2 ? 10300.0 : (C == 4 ? 11200.0 : (C == 8 ? 12200.0 : 16500.0));
+  std::vector<double> d1(n), dC(n);
   for (int e = 0; e < n; ++e) {
     const double sw = (size_t)e < s->env_sweeps.size() ? s->env_sweeps[e] : 1.0;
-    w[e] = s->env_work[e] * std::max(1.0, iters ? std::max((double)iters[e], sw) : sw);
+    const double k = std::max(1.0, iters ? std::max((double)iters[e], sw) : sw);
+    const double slots = s->env_work[e];
+    d1[e] = k * (slots + a1);
+    dC[e] = C > 1 ? k * (slots / C + aC) : d1[e];
   }
   std::vector<int> order(n);
   for (int e = 0; e < n; ++e) order[e] = e;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return d1[a] > d1[b]; });
   work.clear();
   if (C <= 1) {
     for (int e : order) work.push_back(make_int4(e, 0, 1, 0));
@@ -662,30 +675,28 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
     for (int r = 0; r < C; ++r) work.push_back(make_int4(0, r, C, 0));
     return;
   }
-  // parallel efficiency of a split environment (cluster barriers and the
-  // replica broadcasts cost a share of the gain); measured on B200 for a
-  // 68K-slot environment at 512 threads: 129 / 77 / 49 / 36 / 36 us per sweep
-  // on 1 / 2 / 4 / 8 / 16 blocks
-  const double eff = C == 2 ? 0.84 : (C == 4 ? 0.66 : (C == 8 ? 0.45 : 0.22));
   const double cap = std::max(1, s->capacity_blocks);
-  double total = 0.0;
-  for (double x : w) total += x;
+  double area = 0.0;
+  for (double x : d1) area += x;
   int best_h = 0;
-  double best_t = 1e300, extra = 0.0;
+  double best_t = 1e300, t_split = 0.0;
   for (int h = 0; h <= n; ++h) {
-    // the h heaviest environments are split
-    if (h > 0) extra += w[order[h - 1]] * (1.0 / eff - 1.0);
-    const double blocks = (double)(n - h) + (double)h * C;
-    const double t_split = h > 0 ? w[order[0]] / (C * eff) : 0.0;
-    const double t_single = h < n ? w[order[h]] : 0.0;
-    const double t_fill = (total + extra) / std::min(cap, blocks);
-    const double t = std::max(std::max(t_split, t_single), t_fill);
+    // the h longest environments are split
+    if (h > 0) {
+      const int e = order[h - 1];
+      area += C * dC[e] - d1[e];
+      t_split = std::max(t_split, dC[e]);
+    }
+    const double t_single = h < n ? d1[order[h]] : 0.0;
+    const double t = std::max(std::max(t_split, t_single), area / cap);
     if (t < best_t * 0.999) {
       best_t = t;
       best_h = h;
     }
     if (t_single <= t_split) break;  // splitting more cannot help
   }
+  std::stable_sort(order.begin(), order.begin() + best_h,
+                   [&](int a, int b) { return dC[a] > dC[b]; });
   for (int i = 0; i < best_h; ++i)
     for (int r = 0; r < C; ++r) work.push_back(make_int4(order[i], r, C, 0));
   if (s->tiered) {
@@ -1286,7 +1297,7 @@ int finish(vbd_solver* s, int* iters_out) {
     // re-balance the next step from this step's sweep counts (stream is idle)
     s->env_sweeps.resize(s->n_env, 1.0);
     for (int e = 0; e < s->n_env; ++e)
-      s->env_sweeps[e] = std::max((double)s->h_iters[e], 0.9 * s->env_sweeps[e]);
+      s->env_sweeps[e] = std::max((double)s->h_iters[e], 0.95 * s->env_sweeps[e]);
     const int rc = upload_plan(s, s->h_iters);
     if (rc != VBD_OK) return rc;
   }
