@@ -473,10 +473,17 @@ struct vbd_solver {
   bool replan = false;       // re-plan from the measured sweep counts after each step
   int capacity_blocks = 0;   // resident blocks on the device for this launch shape
   std::vector<double> env_work;  // incident slots per environment
-  // sweeps per environment for the plan: max(last step, 0.9 x previous
-  // estimate), so an environment whose sweep count jumps between steps keeps
-  // its share of the device
-  std::vector<double> env_sweeps;
+  // sweeps per environment for the plan.  Plain VBD's counts change slowly
+  // from step to step: env_sweeps_decay = max(last, 0.95 x previous).  The
+  // learned warm start's vary (consecutive-step correlation about 0.7 on the
+  // 256-environment batch): the maximum of the last kSweepWindow counts for
+  // the length of its job (an environment whose count jumps must not run
+  // alone on one block) and their running mean for the total block time;
+  // env_sweep_ring holds the window
+  static constexpr int kSweepWindow = 8;
+  std::vector<double> env_sweeps, env_sweeps_mean, env_sweeps_decay;
+  std::vector<int> env_sweep_ring;
+  int ring_pos = 0;
   std::vector<int4> work;
   DevBuf<int4> d_work;
   // tiered block mode (VBD_TIERED): `work` lists the split environments
@@ -635,9 +642,9 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
 }
 
 // Block-mode work map.  Each environment's duration is predicted from its
-// slot count and its expected sweep count (a slowly decaying maximum of its
-// past counts; 1 before the first step) with a per-sweep cost model measured
-// on B200 at 512 threads, in units of one slot visit of a single block:
+// slot count and its sweep count (1 before the first step) with a per-sweep
+// cost model measured on B200 at 512 threads, in units of one slot visit of
+// a single block:
 //   one block              sweeps * (slots + 8300)
 //   split over C blocks    sweeps * (slots / C + I_C),
 //                          I_C = 10300 / 11200 / 12200 / 16500 for C = 2 / 4 / 8 / 16
@@ -647,21 +654,38 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
 // blocks).  With cluster > 1 the longest environments may each take a whole
 // cluster (group = cluster); the split set is the one with the smallest
 // predicted step time, the largest of (longest split environment, longest
-// single-block environment, all block time / resident blocks).  Blocks are
-// listed longest first, which the block scheduler then starts first.
+// single-block environment, all block time / resident blocks).  With the
+// learned warm start, job lengths use the high sweep estimate (the maximum
+// of the last eight steps) and the total block time the mean, both plus the
+// cost of its energy checks (1.9 sweeps): its counts vary from step to step,
+// and an environment whose count jumps while it runs alone on one block sets
+// the step time.  Blocks are listed longest first, which the block scheduler
+// then starts first.
 void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
                std::vector<int4>& work2) {
   const int n = s->n_env, C = s->cluster;
   work2.clear();
   const double a1 = 8300.0;
   const double aC = C == 2 ? 10300.0 : (C == 4 ? 11200.0 : (C == 8 ? 12200.0 : 16500.0));
-  std::vector<double> d1(n), dC(n);
+  std::vector<double> d1(n), dC(n), m1(n), mC(n);  // high and mean estimates
+  const bool hist = s->env_sweeps.size() == (size_t)n && s->env_sweeps_mean.size() == (size_t)n &&
+                    s->env_sweeps_decay.size() == (size_t)n;
+  // the learned warm start's energy checks cost about 1.9 sweeps (measured)
+  const double kw = s->warm ? 1.9 : 0.0;
   for (int e = 0; e < n; ++e) {
-    const double sw = (size_t)e < s->env_sweeps.size() ? s->env_sweeps[e] : 1.0;
-    const double k = std::max(1.0, iters ? std::max((double)iters[e], sw) : sw);
+    const double last = iters ? (double)iters[e] : 1.0;
+    double k = last, km = last;
+    if (hist) {
+      k = std::max(last, s->warm ? s->env_sweeps[e] : s->env_sweeps_decay[e]);
+      km = s->warm ? s->env_sweeps_mean[e] : k;
+    }
+    k = std::max(1.0, k) + kw;
+    km = std::max(1.0, km) + kw;
     const double slots = s->env_work[e];
     d1[e] = k * (slots + a1);
     dC[e] = C > 1 ? k * (slots / C + aC) : d1[e];
+    m1[e] = km * (slots + a1);
+    mC[e] = C > 1 ? km * (slots / C + aC) : m1[e];
   }
   std::vector<int> order(n);
   for (int e = 0; e < n; ++e) order[e] = e;
@@ -677,14 +701,14 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
   }
   const double cap = std::max(1, s->capacity_blocks);
   double area = 0.0;
-  for (double x : d1) area += x;
+  for (double x : m1) area += x;
   int best_h = 0;
   double best_t = 1e300, t_split = 0.0;
   for (int h = 0; h <= n; ++h) {
     // the h longest environments are split
     if (h > 0) {
       const int e = order[h - 1];
-      area += C * dC[e] - d1[e];
+      area += C * mC[e] - m1[e];
       t_split = std::max(t_split, dC[e]);
     }
     const double t_single = h < n ? d1[order[h]] : 0.0;
@@ -1295,9 +1319,21 @@ int finish(vbd_solver* s, int* iters_out) {
   }
   if (s->replan) {
     // re-balance the next step from this step's sweep counts (stream is idle)
+    const int W = vbd_solver::kSweepWindow;
+    const bool first = s->env_sweeps.empty();
     s->env_sweeps.resize(s->n_env, 1.0);
-    for (int e = 0; e < s->n_env; ++e)
-      s->env_sweeps[e] = std::max((double)s->h_iters[e], 0.95 * s->env_sweeps[e]);
+    s->env_sweeps_mean.resize(s->n_env, 1.0);
+    s->env_sweeps_decay.resize(s->n_env, 1.0);
+    s->env_sweep_ring.resize((size_t)s->n_env * W, 0);
+    for (int e = 0; e < s->n_env; ++e) {
+      const double k = s->h_iters[e];
+      int* ring = &s->env_sweep_ring[(size_t)e * W];
+      ring[s->ring_pos] = s->h_iters[e];
+      s->env_sweeps[e] = *std::max_element(ring, ring + W);
+      s->env_sweeps_mean[e] = first ? k : 0.9 * s->env_sweeps_mean[e] + 0.1 * k;
+      s->env_sweeps_decay[e] = std::max(k, 0.95 * s->env_sweeps_decay[e]);
+    }
+    s->ring_pos = (s->ring_pos + 1) % W;
     const int rc = upload_plan(s, s->h_iters);
     if (rc != VBD_OK) return rc;
   }
