@@ -479,7 +479,8 @@ def run_ours(args, envs, desc, batched):
         cant = scenes.cantilever(160)
         cs = make_solver([cant], False, local,
                          tuned=tuned_config([cant], False, local, "auto", not args.no_tune))
-        cms, cit, _ = timed_steps(cs, False, args.secondary_steps, 3, local, flush)
+        cdet = {}
+        cms, cit, _ = timed_steps(cs, False, args.secondary_steps, 3, local, flush, detail=cdet)
         cb, csolved, _ = sweep_bytes(cant)
         t = float(cms.sum()) * 1e-3
         line["cantilever160"] = {
@@ -487,18 +488,21 @@ def run_ours(args, envs, desc, batched):
             "ms_per_step": 1e3 * t / args.secondary_steps,
             "iters_per_step": float(cit.mean()), "mode": MODE_NAMES[cs.info()["mode"]],
             "vertex_updates_per_s": csolved * float(cit.sum()) / t,
-            "roofline_frac": cb * float(cit.sum()) / t / 1e9 / peak}
+            "roofline_frac": cb * float(cit.sum()) / t / 1e9 / peak,
+            "kernel_ms_per_step": float(np.mean(cdet["kernel_ms"]))}
         cs.close()
         # the same cantilever with the learned warm start (persistent mode)
         from warpvbd_b200 import warmstart
         ws_ = make_solver([cant], False, local, warm=warmstart.load(),
                           tuned=tuned_config([cant], False, local, "auto", not args.no_tune))
-        wms, wit, _ = timed_steps(ws_, False, args.secondary_steps, 3, local, flush)
+        wdet = {}
+        wms, wit, _ = timed_steps(ws_, False, args.secondary_steps, 3, local, flush, detail=wdet)
         tw = float(wms.sum()) * 1e-3
         line["cantilever160_warm_start"] = {
             "sim_s_per_wall_s": args.secondary_steps * DT / tw,
             "ms_per_step": 1e3 * tw / args.secondary_steps,
             "iters_per_step": float(wit.mean()),
+            "kernel_ms_per_step": float(np.mean(wdet["kernel_ms"])),
             "speedup_vs_plain": t / tw}
         ws_.close()
     if world > 1:

@@ -476,6 +476,14 @@ __device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, cons
   const bool valid = gv < ci.vend;
   const int lv = gv - vbase;
   const ChunkInfo ch = m.chunk[q];
+  // slot indices up to the prefetch depth first, as in process_chunk
+  using RS = RawSlot<FMT>;
+  constexpr int PF = Prefetch<TPV>::steps;
+  const size_t base = (size_t)ch.block * 32 + lane;
+  typename RS::type sl[PF];
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps) sl[s] = RS::load(m, base + (size_t)s * 32);
   int k = 0;
   S4 uo;
   uo.x = uo.y = uo.z = uo.w = SReal(0);
@@ -484,20 +492,21 @@ __device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, cons
     uo = st.load(lv);
   }
   double acc = 0.0;
-  const size_t base = (size_t)ch.block * 32 + lane;
-  for (int s = 0; s < ch.steps; ++s) {
-    if (s * TPV + sub < k) {
-      const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
-      const R4* t = tab + 3 * (size_t)id.w;
-      const S4 a = st.load(id.x);
-      const S4 b = st.load(id.y);
-      const S4 c = st.load(id.z);
-      acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
-                                           Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
-                                           Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
-                                           t[0], t[1], t[2]));
-    }
-  }
+  auto visit = [&](const int4& id) {
+    const R4* t = tab + 3 * (size_t)id.w;
+    const S4 a = st.load(id.x);
+    const S4 b = st.load(id.y);
+    const S4 c = st.load(id.z);
+    acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                                         Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                                         Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
+                                         t[0], t[1], t[2]));
+  };
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps && s * TPV + sub < k) visit(RS::unpack(sl[s]));
+  for (int s = PF; s < ch.steps; ++s)
+    if (s * TPV + sub < k) visit(load_slot<FMT>(m, base + (size_t)s * 32));
   if (inertia && valid && sub == 0) {
     const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
     const double dx = double(uo.x - tt.x), dy = double(uo.y - tt.y), dz = double(uo.z - tt.z);
@@ -535,6 +544,14 @@ __device__ __forceinline__ double2 energy_chunk_pair(const DevMesh& m, int vbase
     }
     return v;
   };
+  // slot indices up to the prefetch depth first, as in process_chunk
+  using RS = RawSlot<FMT>;
+  constexpr int PF = Prefetch<TPV>::steps;
+  const size_t base = (size_t)ch.block * 32 + lane;
+  typename RS::type sl[PF];
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps) sl[s] = RS::load(m, base + (size_t)s * 32);
   int k = 0;
   S4 uo, uob;
   uo.x = uo.y = uo.z = uo.w = SReal(0);
@@ -545,26 +562,27 @@ __device__ __forceinline__ double2 energy_chunk_pair(const DevMesh& m, int vbase
     uob = shifted(uo, lv);
   }
   double acc = 0.0, accb = 0.0;
-  const size_t base = (size_t)ch.block * 32 + lane;
-  for (int s = 0; s < ch.steps; ++s) {
-    if (s * TPV + sub < k) {
-      const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
-      const R4* t = tab + 3 * (size_t)id.w;
-      const R4 q0 = t[0], q1 = t[1], q2 = t[2];
-      const S4 a = st.load(id.x);
-      const S4 b = st.load(id.y);
-      const S4 c = st.load(id.z);
-      acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
-                                           Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
-                                           Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
-                                           q0, q1, q2));
-      const S4 ab = shifted(a, id.x), bb = shifted(b, id.y), cb = shifted(c, id.z);
-      accb += double(slot_energy<Real, MAT>(
-          Real(ab.x - uob.x), Real(ab.y - uob.y), Real(ab.z - uob.z), Real(bb.x - uob.x),
-          Real(bb.y - uob.y), Real(bb.z - uob.z), Real(cb.x - uob.x), Real(cb.y - uob.y),
-          Real(cb.z - uob.z), q0, q1, q2));
-    }
-  }
+  auto visit = [&](const int4& id) {
+    const R4* t = tab + 3 * (size_t)id.w;
+    const R4 q0 = t[0], q1 = t[1], q2 = t[2];
+    const S4 a = st.load(id.x);
+    const S4 b = st.load(id.y);
+    const S4 c = st.load(id.z);
+    const S4 ab = shifted(a, id.x), bb = shifted(b, id.y), cb = shifted(c, id.z);
+    acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                                         Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                                         Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
+                                         q0, q1, q2));
+    accb += double(slot_energy<Real, MAT>(
+        Real(ab.x - uob.x), Real(ab.y - uob.y), Real(ab.z - uob.z), Real(bb.x - uob.x),
+        Real(bb.y - uob.y), Real(bb.z - uob.z), Real(cb.x - uob.x), Real(cb.y - uob.y),
+        Real(cb.z - uob.z), q0, q1, q2));
+  };
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps && s * TPV + sub < k) visit(RS::unpack(sl[s]));
+  for (int s = PF; s < ch.steps; ++s)
+    if (s * TPV + sub < k) visit(load_slot<FMT>(m, base + (size_t)s * 32));
   if (valid && sub == 0) {
     const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
     const double dx = double(uob.x - tt.x), dy = double(uob.y - tt.y), dz = double(uob.z - tt.z);

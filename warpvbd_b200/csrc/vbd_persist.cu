@@ -168,17 +168,10 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
   unsigned stat = 0u;
   if (pp->warm && m.ws_pred) {
     const S4* UT = reinterpret_cast<const S4*>(m.ut) + e.vbase;
-    // grid-wide incremental potential of the current U, partial sums in
-    // parts[slot * nb + block]
-    auto grid_energy = [&](bool inertia, int slot, bool& ok) -> double {
-      double acc = 0.0;
-      for (int c = 0; c < e.ncolors; ++c) {
-        const ColorInfo ci = m.color[e.cbase + c];
-        for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
-             q += nb * nwarps)
-          acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc,
-                                                          inertia, tab);
-      }
+    // grid-wide sums of per-block partials: each block writes its partial to
+    // parts[slot * nb + block]; after a barrier every block adds them in block
+    // order, so all blocks see the same total
+    auto grid_sum = [&](double acc, int slot, bool& ok) -> double {
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
       if (lane == 0) s_dsum[warp] = acc;
@@ -196,13 +189,23 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
         s_total = v;
       }
       __syncthreads();
-      return s_total;
+      const double total = s_total;
+      __syncthreads();  // s_total is reused by the next sum
+      return total;
     };
-    bool ok = true;
-    const double e0 = grid_energy(false, 0, ok);
-    bool used = false;
-    for (int trial = 0; trial < 3 && ok && !used; ++trial) {
-      const SReal alpha = SReal(1.0 / double(1 << trial));
+    // incremental potential of the current U
+    auto grid_energy = [&](bool inertia, int slot, bool& ok) -> double {
+      double acc = 0.0;
+      for (int c = 0; c < e.ncolors; ++c) {
+        const ColorInfo ci = m.color[e.cbase + c];
+        for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
+             q += nb * nwarps)
+          acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc,
+                                                          inertia, tab);
+      }
+      return grid_sum(acc, slot, ok);
+    };
+    auto place = [&](SReal alpha) {
       for (int i = tid; i < e.nsolved; i += nthreads) {
         const float4 d = m.ws_pred[e.vbase + i];
         if (d.w > 0.f) {
@@ -213,11 +216,41 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
           U[e.vbase + i] = v;
         }
       }
+    };
+    // the potential at the inertia guess (U) and at the full prediction in
+    // one pass (energy_chunk_pair forms the shifted positions exactly as
+    // place(1) stores them, so both sums equal separate passes bit for bit)
+    bool ok = true;
+    double e0, e1;
+    {
+      double a0 = 0.0, a1 = 0.0;
+      for (int c = 0; c < e.ncolors; ++c) {
+        const ColorInfo ci = m.color[e.cbase + c];
+        for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
+             q += nb * nwarps) {
+          const double2 p2 =
+              energy_chunk_pair<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, tab);
+          a0 += p2.x;
+          a1 += p2.y;
+        }
+      }
+      e0 = grid_sum(a0, 0, ok);
+      e1 = ok ? grid_sum(a1, 1, ok) : 0.0;
+    }
+    bool used = ok && e1 < e0;  // false on NaN as well
+    if (used) {
+      place(SReal(1));
+      bar += nb;
+      ok = grid_sync(ctl, bar, lim, &s_ok);
+    }
+    // backtracking: half and a quarter of the prediction
+    for (int trial = 1; trial < 3 && ok && !used; ++trial) {
+      place(SReal(1.0 / double(1 << trial)));
       bar += nb;
       ok = grid_sync(ctl, bar, lim, &s_ok);
       if (!ok) break;
-      const double e1 = grid_energy(true, 1 + trial, ok);
-      used = ok && e1 < e0;  // false on NaN as well
+      const double et = grid_energy(true, 1 + trial, ok);
+      used = ok && et < e0;
     }
     if (!ok) {
       if (threadIdx.x == 0) atomicOr(m.status, kStatTimeout);
