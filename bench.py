@@ -160,6 +160,14 @@ def clocks_stop(p, gpu_index):
             "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
+def sweep_histogram(iters):
+    """Sweep counts of every (environment, step) pair in power-of-two bins:
+    counts[i] holds the pairs with edges[i] <= sweeps < edges[i + 1]."""
+    edges = [1, 2, 4, 8, 16, 32, 64, 128, 256, 512, MAX_ITER + 1]
+    counts, _ = np.histogram(np.asarray(iters).reshape(-1), bins=edges)
+    return {"edges": edges, "counts": counts.tolist()}
+
+
 def measured_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -199,12 +207,12 @@ def concat(envs):
                 poissons_ratio=np.concatenate(nu), active_mask=np.concatenate(act))
 
 
-def oracle_rate(envs, budget_s, max_steps, warmup=0):
-    """The FP64 oracle (OpenMP on all host threads) stepping `envs` as one
-    concatenated mesh, as the reference batches; returns (env-sim-s per wall-s,
-    steps, threads)."""
+def oracle_rate(envs, budget_s, max_steps, warmup=0, threads=None):
+    """The FP64 oracle (OpenMP on all host threads, or `threads`) stepping
+    `envs` as one concatenated mesh, as the reference batches; returns
+    (env-sim-s per wall-s, steps, threads, seconds)."""
     from oracle import oracle
-    n = oracle.max_threads()
+    n = threads or oracle.max_threads()
     oracle.set_threads(n)
     o = oracle.OracleSolver(**concat(envs), damping_coefficient=0.0, dx_tol=TOL,
                             max_iter=MAX_ITER, guarded=True)
@@ -410,7 +418,8 @@ def run_ours(args, envs, desc, batched):
                        "autotuned": tuned is not None,
                        "tiered": bool((tuned or {}).get("tiered", False)),
                        "l2": "256 MiB written between timed steps"},
-            "iters_per_step": {"mean": float(iters.mean()), "max": int(iters.max()),
+            "iters_per_step": {"hist": sweep_histogram(iters),
+                               "mean": float(iters.mean()), "max": int(iters.max()),
                                "min": int(iters.min())},
             "vertex_updates_per_s": world * float((iters * solved[None, :]).sum())
             / (total_ms * 1e-3),
@@ -433,6 +442,11 @@ def run_ours(args, envs, desc, batched):
             "sample": f"{k} whole steps of {len(sample)} environment(s) "
                       + ("concatenated into one mesh " if batched else "")
                       + f"({el:.1f} s), FP64 C oracle, OpenMP {n} threads"}
+        # the reference's Warp CPU device runs its kernels on one thread: the
+        # same oracle on one thread, one environment, a few seconds
+        v1, k1, _, el1 = oracle_rate(sample[:1], min(5.0, args.cpu_budget_s), 50, threads=1)
+        line["cpu_baseline"]["single_thread"] = {
+            "value": v1, "sample": f"{k1} whole steps of 1 environment ({el1:.1f} s), 1 thread"}
     if batched and not args.no_secondary:
         # the same batch with the learned warm start toggled (same timing
         # method); every rank takes this path, so the collectives match
@@ -455,7 +469,8 @@ def run_ours(args, envs, desc, batched):
         pinfo = ps.info()
         line[key] = {
             "value": pv, "ms_per_step": pt / args.steps,
-            "iters_per_step": {"mean": float(pit.mean()), "max": int(pit.max())},
+            "iters_per_step": {"mean": float(pit.mean()), "max": int(pit.max()),
+                               "hist": sweep_histogram(pit)},
             "roofline_frac": pbytes / (pt * 1e-3) / 1e9 / peak,
             "shape": {"tpv": pinfo["tpv"], "block_threads": pinfo["block_threads"],
                       "cluster": pinfo["cluster"]}}

@@ -64,3 +64,20 @@ def test_committed_table_is_valid_json():
         d = json.load(open(autotune.PACKAGE_TABLE))
         for ent in d.values():
             assert ent["config"]["tpv"] in (0, 2, 4, 8, 16)
+
+
+def test_timeline_summary_on_a_synthetic_trace():
+    """The step-timeline report: blocks per SM from overlapping records, the
+    busy fraction and the per-class cost, on a hand-made two-SM trace."""
+    import numpy as np
+    from warpvbd_b200 import timeline
+    tl = {"start_ns": np.array([0, 0, 50, 0]), "end_ns": np.array([100, 50, 100, 100]),
+          "env": np.array([0, 1, 2, 3]), "rank": np.array([0, 0, 0, 0]),
+          "sm": np.array([0, 1, 1, 0]), "sweeps": np.array([2, 1, 1, 1]),
+          "launch": np.array([1, 1, 1, 1])}
+    assert timeline.blocks_per_sm(tl) == 2
+    assert timeline.busy_fraction(tl, 4) == 300 / 400
+    rows, cost = timeline.summarize([{"timeline": tl, "iters": np.array([2, 1, 1, 1]),
+                                      "kernel_ms": 0.1}], np.array([10.0, 5, 5, 10]), 4)
+    assert rows[0]["blocks"] == 4 and rows[0]["last"][0] in (0, 2, 3)
+    assert abs(cost["single"] - 300 / (20 + 5 + 5 + 10)) < 1e-12

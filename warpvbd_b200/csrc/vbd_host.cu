@@ -9,6 +9,7 @@
 // vertices colour by colour and stores one record per incident (vertex, tet)
 // pair in a SELL-32 layout (see vbd_internal.h).
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -621,6 +622,15 @@ void free_solver(vbd_solver* s) {
   delete s;
 }
 
+// NVTX range over a host-side scope (header-only NVTX v3: a no-op unless a
+// profiler is attached).  Names: "vbd_step" (enqueue, and the wait when the
+// call blocks), "vbd_warm_start" (feature and inference launches),
+// "vbd_step_kernels" (the step launches), "vbd_sync".
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int d) {
@@ -1197,6 +1207,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
     if (s->cur_params.trace)
       CUDA_TRY(cudaMemsetAsync(s->d_trace.p, 0, sizeof(unsigned long long) * s->d_trace.n, st));
     if (s->warm) {
+      NvtxRange nw("vbd_warm_start");
       // features of the coming step, then the network's predicted corrections
       CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
                                   s->ws_history ? 1 : 0, s->d_wpack.p, s->d_feat.p, st));
@@ -1205,6 +1216,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
       launches += 3;  // pack, features, inference
     }
     CUDA_TRY(cudaEventRecord(s->ev_k0, st));
+    NvtxRange nk("vbd_step_kernels");
     if (!s->tiered) {
       ++launches;
       CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
@@ -1234,6 +1246,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
     }
   } else if (s->mode == VBD_MODE_PERSIST) {
     if (s->warm) {
+      NvtxRange nw("vbd_warm_start");
       CUDA_TRY(launch_ws_features(s->prec, s->tpv, m, (int)s->L.chunk.size(), dt, s->g,
                                   s->ws_history ? 1 : 0, s->d_wpack.p, s->d_feat.p, st));
       CUDA_TRY(launch_ws_infer(s->d_feat.p, s->V, s->d_wbf.p, s->d_wnorm.p, s->d_wstat.p,
@@ -1241,6 +1254,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
       launches += 3;
     }
     CUDA_TRY(cudaEventRecord(s->ev_k0, st));
+    NvtxRange nk("vbd_step_kernels");
     ++launches;
     CUDA_TRY(launch_persist(s->prec, s->material, s->tpv, s->threads, m, s->d_params.p,
                             s->d_pctl.p, s->persist_blocks, s->wait_limits, s->d_pparts.p,
@@ -1476,6 +1490,7 @@ int vbd_reset(vbd_solver* s) {
 
 int vbd_step(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out) {
   if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  NvtxRange nr("vbd_step");
   DeviceGuard dg(s->device);
   int rc = enqueue_step(s, dt, tol, nullptr, max_iter);
   if (rc != VBD_OK) return rc;
@@ -1486,6 +1501,7 @@ int vbd_step(vbd_solver* s, double dt, double tol, int max_iter, int* iterations
 int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per_env,
                      int max_iter, int* iterations_out) {
   if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  NvtxRange nr("vbd_step");
   DeviceGuard dg(s->device);
   if (tol_per_env && s->mode != VBD_MODE_BLOCK)
     return fail(VBD_ERR_UNSUPPORTED, "per-environment tolerances need block mode");
@@ -1497,6 +1513,7 @@ int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per
 
 int vbd_sync(vbd_solver* s) {
   if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
+  NvtxRange nr("vbd_sync");
   DeviceGuard dg(s->device);
   if (!s->pending) {
     CUDA_TRY(cudaStreamSynchronize(s->stream));
