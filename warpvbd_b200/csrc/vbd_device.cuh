@@ -408,8 +408,9 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
 }
 
 // ---------------------------------------------------------------------------
-// Incremental potential.  Per slot: the slot's share (q2.w) of the tet's
-// strain energy V psi(F), with the same G as slot_accumulate:
+// Incremental potential.  Strain energy V psi(F) of one tet from one of its
+// slots (any vertex of the tet gives the same F), with the same G as
+// slot_accumulate:
 //   SNH   psi = mu'/2 (Ic-3) - mu'/2 ln((Ic+1)/4) + lambda'/2 (J-alpha)^2
 //   StVK  psi = mu E:E + lambda/2 tr(E)^2
 // (the SNH form differs from mu'/2 (Ic-3) - mu'/2 ln(Ic+1) + ... by a
@@ -417,10 +418,10 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
 // compare two configurations, so constants cancel.
 // ---------------------------------------------------------------------------
 template <typename Real, int MAT>
-__device__ __forceinline__ Real slot_energy(Real d0x, Real d0y, Real d0z, Real d1x, Real d1y,
-                                            Real d1z, Real d2x, Real d2y, Real d2z,
-                                            const real4<Real>& q0, const real4<Real>& q1,
-                                            const real4<Real>& q2) {
+__device__ __forceinline__ Real slot_psi(Real d0x, Real d0y, Real d0z, Real d1x, Real d1y,
+                                         Real d1z, Real d2x, Real d2y, Real d2z,
+                                         const real4<Real>& q0, const real4<Real>& q1,
+                                         const real4<Real>& q2) {
   const Real G00 = d0x * q0.x + d1x * q1.x + d2x * q2.x;
   const Real G01 = d0x * q0.y + d1x * q1.y + d2x * q2.y;
   const Real G02 = d0x * q0.z + d1x * q1.z + d2x * q2.z;
@@ -430,7 +431,7 @@ __device__ __forceinline__ Real slot_energy(Real d0x, Real d0y, Real d0z, Real d
   const Real G20 = d0z * q0.x + d1z * q1.x + d2z * q2.x;
   const Real G21 = d0z * q0.y + d1z * q1.y + d2z * q2.y;
   const Real G22 = d0z * q0.z + d1z * q1.z + d2z * q2.z;
-  const Real p0 = q0.w, p1 = q1.w, w = q2.w;
+  const Real p0 = q0.w, p1 = q1.w;
   const Real t = G00 + G11 + G22;
   Real psi;
   if (MAT == kSNH) {
@@ -458,85 +459,24 @@ __device__ __forceinline__ Real slot_energy(Real d0x, Real d0y, Real d0z, Real d
                     Real(2) * (E01 * E01 + E02 * E02 + E12 * E12);
     psi = p0 * EE + Real(0.5) * p1 * trE * trE;
   }
-  return w * psi;
+  return psi;
 }
 
-// Energy of one chunk's vertices at the state `st`: strain-energy shares of
-// their slots plus, with inertia, m/(2 dt^2) |u - ut|^2 per vertex.
-template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
-__device__ __forceinline__ double energy_chunk(const DevMesh& m, int vbase, const ColorInfo& ci,
-                                               int q, int lane, const State& st,
-                                               const StepConst& sc, bool inertia,
-                                               const real4<Real>* tab) {
+// Strain energies of the environment's tets (its tet list: one owner slot per
+// tet with a solved vertex, the slot's G taken relative to the owner, the
+// energy counted once at full weight), for the entries first, first + stride,
+// ...: x = at the state `st`, y (when `pair`) = at the state shifted by the
+// predicted correction (DevMesh::ws_pred, where w > 0).  The shifted
+// positions are formed exactly as the warm-start stage stores them (state +
+// correction in the state precision).
+template <typename Real, typename SReal, int MAT, class State>
+__device__ __forceinline__ double2 tet_energy(const DevMesh& m, const EnvInfo& e,
+                                              const State& st, const real4<Real>* tab,
+                                              int first, int stride, bool pair) {
   using R4 = real4<Real>;
   using S4 = real4<SReal>;
-  constexpr int CPW = 32 / TPV;
-  const int vi = lane / TPV, sub = lane % TPV;
-  const int gv = ci.vbegin + (q - ci.chunk_begin) * CPW + vi;
-  const bool valid = gv < ci.vend;
-  const int lv = gv - vbase;
-  const ChunkInfo ch = m.chunk[q];
-  // slot indices up to the prefetch depth first, as in process_chunk
-  using RS = RawSlot<FMT>;
-  constexpr int PF = Prefetch<TPV>::steps;
-  const size_t base = (size_t)ch.block * 32 + lane;
-  typename RS::type sl[PF];
-#pragma unroll
-  for (int s = 0; s < PF; ++s)
-    if (s < ch.steps) sl[s] = RS::load(m, base + (size_t)s * 32);
-  int k = 0;
-  S4 uo;
-  uo.x = uo.y = uo.z = uo.w = SReal(0);
-  if (valid) {
-    k = __ldg(m.valence + gv);
-    uo = st.load(lv);
-  }
-  double acc = 0.0;
-  auto visit = [&](const int4& id) {
-    const R4* t = tab + 3 * (size_t)id.w;
-    const S4 a = st.load(id.x);
-    const S4 b = st.load(id.y);
-    const S4 c = st.load(id.z);
-    acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
-                                         Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
-                                         Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
-                                         t[0], t[1], t[2]));
-  };
-#pragma unroll
-  for (int s = 0; s < PF; ++s)
-    if (s < ch.steps && s * TPV + sub < k) visit(RS::unpack(sl[s]));
-  for (int s = PF; s < ch.steps; ++s)
-    if (s * TPV + sub < k) visit(load_slot<FMT>(m, base + (size_t)s * 32));
-  if (inertia && valid && sub == 0) {
-    const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
-    const double dx = double(uo.x - tt.x), dy = double(uo.y - tt.y), dz = double(uo.z - tt.z);
-    acc += 0.5 * double(tt.w) * sc.inv_dt2 * (dx * dx + dy * dy + dz * dz);
-  }
-  return acc;
-}
-
-// Both potentials the learned warm start compares, in one pass over the
-// slots: (x) the elastic energy of the current state (the inertia guess, whose
-// inertia term is zero) and (y) the incremental potential of the state shifted
-// by the predicted correction (DevMesh::ws_pred, where w > 0), inertia term
-// included.  The shifted positions are formed exactly as the warm-start stage
-// stores them (state + correction in the state precision), so (y) equals the
-// potential a separate pass over the shifted state would give, bit for bit.
-template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
-__device__ __forceinline__ double2 energy_chunk_pair(const DevMesh& m, int vbase,
-                                                     const ColorInfo& ci, int q, int lane,
-                                                     const State& st, const StepConst& sc,
-                                                     const real4<Real>* tab) {
-  using R4 = real4<Real>;
-  using S4 = real4<SReal>;
-  constexpr int CPW = 32 / TPV;
-  const int vi = lane / TPV, sub = lane % TPV;
-  const int gv = ci.vbegin + (q - ci.chunk_begin) * CPW + vi;
-  const bool valid = gv < ci.vend;
-  const int lv = gv - vbase;
-  const ChunkInfo ch = m.chunk[q];
   auto shifted = [&](S4 v, int local_id) {
-    const float4 d = m.ws_pred[vbase + local_id];
+    const float4 d = m.ws_pred[e.vbase + local_id];
     if (d.w > 0.f) {
       v.x += SReal(d.x);
       v.y += SReal(d.y);
@@ -544,51 +484,57 @@ __device__ __forceinline__ double2 energy_chunk_pair(const DevMesh& m, int vbase
     }
     return v;
   };
-  // slot indices up to the prefetch depth first, as in process_chunk
-  using RS = RawSlot<FMT>;
-  constexpr int PF = Prefetch<TPV>::steps;
-  const size_t base = (size_t)ch.block * 32 + lane;
-  typename RS::type sl[PF];
-#pragma unroll
-  for (int s = 0; s < PF; ++s)
-    if (s < ch.steps) sl[s] = RS::load(m, base + (size_t)s * 32);
-  int k = 0;
-  S4 uo, uob;
-  uo.x = uo.y = uo.z = uo.w = SReal(0);
-  uob = uo;
-  if (valid) {
-    k = __ldg(m.valence + gv);
-    uo = st.load(lv);
-    uob = shifted(uo, lv);
-  }
   double acc = 0.0, accb = 0.0;
-  auto visit = [&](const int4& id) {
+  for (int i = first; i < e.ntets; i += stride) {
+    const int4 id = __ldg(m.tet_slot + e.tbase + i);
+    const int o = __ldg(m.tet_owner + e.tbase + i);
     const R4* t = tab + 3 * (size_t)id.w;
     const R4 q0 = t[0], q1 = t[1], q2 = t[2];
+    const S4 uo = st.load(o);
     const S4 a = st.load(id.x);
     const S4 b = st.load(id.y);
     const S4 c = st.load(id.z);
-    const S4 ab = shifted(a, id.x), bb = shifted(b, id.y), cb = shifted(c, id.z);
-    acc += double(slot_energy<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
-                                         Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
-                                         Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z),
-                                         q0, q1, q2));
-    accb += double(slot_energy<Real, MAT>(
-        Real(ab.x - uob.x), Real(ab.y - uob.y), Real(ab.z - uob.z), Real(bb.x - uob.x),
-        Real(bb.y - uob.y), Real(bb.z - uob.z), Real(cb.x - uob.x), Real(cb.y - uob.y),
-        Real(cb.z - uob.z), q0, q1, q2));
-  };
-#pragma unroll
-  for (int s = 0; s < PF; ++s)
-    if (s < ch.steps && s * TPV + sub < k) visit(RS::unpack(sl[s]));
-  for (int s = PF; s < ch.steps; ++s)
-    if (s * TPV + sub < k) visit(load_slot<FMT>(m, base + (size_t)s * 32));
-  if (valid && sub == 0) {
-    const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
-    const double dx = double(uob.x - tt.x), dy = double(uob.y - tt.y), dz = double(uob.z - tt.z);
-    accb += 0.5 * double(tt.w) * sc.inv_dt2 * (dx * dx + dy * dy + dz * dz);
+    acc += double(slot_psi<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                                      Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                                      Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z), q0,
+                                      q1, q2));
+    if (pair) {
+      const S4 uob = shifted(uo, o);
+      const S4 ab = shifted(a, id.x), bb = shifted(b, id.y), cb = shifted(c, id.z);
+      accb += double(slot_psi<Real, MAT>(
+          Real(ab.x - uob.x), Real(ab.y - uob.y), Real(ab.z - uob.z), Real(bb.x - uob.x),
+          Real(bb.y - uob.y), Real(bb.z - uob.z), Real(cb.x - uob.x), Real(cb.y - uob.y),
+          Real(cb.z - uob.z), q0, q1, q2));
+    }
   }
   return make_double2(acc, accb);
+}
+
+// Inertia energies m/(2 dt^2) |x - ut|^2 of the environment's solved
+// vertices first, first + stride, ...: x = the state `st`, or (shifted) the
+// state plus the predicted correction.
+template <typename SReal, class State>
+__device__ __forceinline__ double inertia_energy(const DevMesh& m, const EnvInfo& e,
+                                                 const State& st, const StepConst& sc,
+                                                 int first, int stride, bool shifted) {
+  using S4 = real4<SReal>;
+  double acc = 0.0;
+  for (int i = first; i < e.nsolved; i += stride) {
+    S4 u = st.load(i);
+    if (shifted) {
+      const float4 d = m.ws_pred[e.vbase + i];
+      if (d.w > 0.f) {
+        u.x += SReal(d.x);
+        u.y += SReal(d.y);
+        u.z += SReal(d.z);
+      }
+    }
+    // ut is written in this launch by another block of a group: through L2
+    const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + e.vbase + i);
+    const double dx = double(u.x - tt.x), dy = double(u.y - tt.y), dz = double(u.z - tt.z);
+    acc += 0.5 * double(tt.w) * sc.inv_dt2 * (dx * dx + dy * dy + dz * dz);
+  }
+  return acc;
 }
 
 // Inertia target and initial guess (position_initialization,

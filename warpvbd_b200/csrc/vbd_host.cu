@@ -205,6 +205,8 @@ struct Layout {
   std::vector<ColorInfo> color;
   std::vector<ChunkInfo> chunk;
   std::vector<int4> rec_idx;  // (n0, n1, n2, record id)
+  std::vector<int4> tet_slot;  // owner slot of every tet with a solved vertex
+  std::vector<int> tet_owner;  // its owner's environment-local id
   RecordTable table;
   std::vector<int> valence;     // new id
   std::vector<double> mass;     // new id
@@ -383,6 +385,7 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
     L.rec_idx.resize((size_t)block_count * 32, make_int4(0, 0, 0, 0));
     RecordTable etab;
     etab.fp64 = L.table.fp64;
+    std::vector<std::pair<int, int4>> tlist;  // (owner, owner slot) per tet
     std::vector<int> old_of_new_local(vn);
     for (int v = 0; v < vn; ++v) old_of_new_local[new_local[v]] = v;
     for (int ci_i = ei.cbase; ci_i < ei.cbase + ei.ncolors; ++ci_i) {
@@ -405,9 +408,13 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
             double val[12];
             const double* bt = &td.b[(size_t)t * 12];
             const double* pt = &td.p[(size_t)t * 3];
-            int n = 0, solved_in_tet = 0;
+            int n = 0, solved_in_tet = 0, owner = vn;
             for (int qq = 0; qq < 4; ++qq) {
-              if (new_local[tets[4 * (size_t)t + qq] - vo] < ei.nsolved) ++solved_in_tet;
+              const int nl = new_local[tets[4 * (size_t)t + qq] - vo];
+              if (nl < ei.nsolved) {
+                ++solved_in_tet;
+                owner = std::min(owner, nl);
+              }
               if (qq == a) continue;
               ids[n] = new_local[tets[4 * (size_t)t + qq] - vo];
               val[4 * n + 0] = bt[qq * 3 + 0];
@@ -422,6 +429,7 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
             val[11] = 1.0 / solved_in_tet;
             const int rid = etab.insert(val);
             L.rec_idx[blk * 32 + lane] = make_int4(ids[0], ids[1], ids[2], rid);
+            if (owner == gv - vo) tlist.emplace_back(owner, make_int4(ids[0], ids[1], ids[2], rid));
             L.n_slots++;
           }
         }
@@ -429,6 +437,17 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
     }
     L.env.back().rbase = L.table.size();
     L.env.back().nrec = etab.size();
+    // the tet list in owner order (neighbouring entries read nearby state)
+    std::stable_sort(tlist.begin(), tlist.end(),
+                     [](const std::pair<int, int4>& a, const std::pair<int, int4>& b) {
+                       return a.first < b.first;
+                     });
+    L.env.back().tbase = (int)L.tet_slot.size();
+    L.env.back().ntets = (int)tlist.size();
+    for (const auto& x : tlist) {
+      L.tet_owner.push_back(x.first);
+      L.tet_slot.push_back(x.second);
+    }
     L.table.vals.insert(L.table.vals.end(), etab.vals.begin(), etab.vals.end());
     L.max_env_records = std::max(L.max_env_records, etab.size());
   }
@@ -457,6 +476,8 @@ struct vbd_solver {
   DevBuf<ChunkInfo> d_chunk;
   DevBuf<int4> d_rec_idx;
   DevBuf<ushort4> d_rec_idx16;
+  DevBuf<int4> d_tet_slot;
+  DevBuf<int> d_tet_owner;
   DevBuf<unsigned char> d_rec_tab;
   int fmt = kFmtIdx32;
   DevBuf<int> d_valence, d_map, d_iters;
@@ -544,6 +565,8 @@ struct vbd_solver {
     m.rec_idx = d_rec_idx.p;
     m.rec_idx16 = d_rec_idx16.p;
     m.rec_tab = d_rec_tab.p;
+    m.tet_slot = d_tet_slot.p;
+    m.tet_owner = d_tet_owner.p;
     m.fmt = fmt;
     m.wstat = d_wstat.p;
     m.chunk_owner = d_chunk_owner.p;
@@ -576,6 +599,8 @@ void free_solver(vbd_solver* s) {
   s->d_chunk.release();
   s->d_rec_idx.release();
   s->d_rec_idx16.release();
+  s->d_tet_slot.release();
+  s->d_tet_owner.release();
   s->d_rec_tab.release();
   s->d_valence.release();
   s->d_map.release();
@@ -974,6 +999,8 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     if (!err) cudaStreamSynchronize(st);  // staging vectors go out of scope
   }
   if (!err && bad(s->d_valence.upload(L.valence, st), "valence")) err = 1;
+  if (!err && bad(s->d_tet_slot.upload(L.tet_slot, st), "tet list")) err = 1;
+  if (!err && bad(s->d_tet_owner.upload(L.tet_owner, st), "tet owners")) err = 1;
   if (!err && bad(s->d_map.upload(L.new_of_old, st), "map")) err = 1;
   if (!err) {
     std::vector<float4> ws(V);
@@ -1097,6 +1124,7 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
                                  s->d_rec_idx16.n * sizeof(ushort4) + s->d_rec_tab.n);
   s->device_bytes += (long long)(4 * sb + s->d_X.n * 8 + s->d_io.n * 8);
   s->device_bytes += (long long)(s->d_valence.n * 4 + s->d_map.n * 4);
+  s->device_bytes += (long long)(s->d_tet_slot.n * sizeof(int4) + s->d_tet_owner.n * 4);
   *out = s;
   return VBD_OK;
 }

@@ -50,6 +50,8 @@ struct EnvInfo {
   int ncolors;
   int rbase;    // first record of the environment's record table (3 Real4 each)
   int nrec;     // records of the environment (slot record ids are environment-local)
+  int tbase;    // first entry of the environment's tet list (DevMesh::tet_slot)
+  int ntets;    // tets with a solved vertex
 };
 
 struct ColorInfo {
@@ -95,6 +97,10 @@ struct DevMesh {
   const int4* rec_idx;       // kFmtIdx32 slots
   const ushort4* rec_idx16;  // kFmtIdx16 slots
   const void* rec_tab;       // Real4 [n_unique][3]
+  // per tet with a solved vertex, for the incremental potential: the slot of
+  // its owner (its solved vertex of lowest local id) and the owner's local id
+  const int4* tet_slot;
+  const int* tet_owner;
   const int* valence;   // per global vertex
   void* u;              // Real4
   void* ut;

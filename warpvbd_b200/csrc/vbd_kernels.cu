@@ -141,21 +141,18 @@ __device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, co
   }
 }
 
-// Incremental potential of an environment at its block's replica, summed over
-// the group: every block sums its share of the chunks, the block sums are
-// exchanged through distributed shared memory (slot `buf` of s_esum).
-template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
+// Incremental potential of an environment at its block's replica (tets'
+// strain energy plus the solved vertices' inertia energy), summed over the
+// group: every block sums its share of the tets and vertices, the block sums
+// are exchanged through distributed shared memory (slot `buf` of s_esum).
+template <typename Real, typename SReal, int MAT, bool GROUP>
 __device__ double env_energy(const DevMesh& m, const EnvInfo& e, const SmemState<SReal>& st,
-                             int rank, int g, const StepConst& sc, bool inertia, double* s_sum,
+                             int rank, int g, const StepConst& sc, double* s_sum,
                              double (*s_esum)[kMaxGroup], int buf, const real4<Real>* tab) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  double acc = 0.0;
-  for (int c = 0; c < e.ncolors; ++c) {
-    const ColorInfo ci = m.color[e.cbase + c];
-    for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
-      acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, st, sc, inertia,
-                                                      tab);
-  }
+  const int first = rank * blockDim.x + threadIdx.x, stride = g * blockDim.x;
+  double acc = tet_energy<Real, SReal, MAT>(m, e, st, tab, first, stride, false).x;
+  acc += inertia_energy<SReal>(m, e, st, sc, first, stride, false);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
   if (lane == 0) s_sum[warp] = acc;
@@ -182,25 +179,20 @@ __device__ double env_energy(const DevMesh& m, const EnvInfo& e, const SmemState
   return v;
 }
 
-// Both potentials of energy_chunk_pair summed over the environment (and the
-// group): x = at the inertia guess, y = at inertia guess + predicted
-// correction.  Block sums are exchanged through distributed shared memory in
-// s_pair (one slot per rank).
-template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
+// Both potentials the learned warm start compares, in one pass, summed over
+// the environment (and the group): x = the strain energy at the inertia guess
+// (its inertia energy is zero), y = the incremental potential at inertia guess
+// + predicted correction.  Block sums are exchanged through distributed
+// shared memory in s_pair (one slot per rank).
+template <typename Real, typename SReal, int MAT, bool GROUP>
 __device__ double2 env_energy_pair(const DevMesh& m, const EnvInfo& e, const SmemState<SReal>& st,
                                    int rank, int g, const StepConst& sc, double* s_sum,
                                    double2* s_pair, const real4<Real>* tab) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  double a = 0.0, b = 0.0;
-  for (int c = 0; c < e.ncolors; ++c) {
-    const ColorInfo ci = m.color[e.cbase + c];
-    for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps) {
-      const double2 v = energy_chunk_pair<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, st,
-                                                                       sc, tab);
-      a += v.x;
-      b += v.y;
-    }
-  }
+  const int first = rank * blockDim.x + threadIdx.x, stride = g * blockDim.x;
+  const double2 el = tet_energy<Real, SReal, MAT>(m, e, st, tab, first, stride, true);
+  double a = el.x;
+  double b = el.y + inertia_energy<SReal>(m, e, st, sc, first, stride, true);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, off);
@@ -247,8 +239,9 @@ __device__ double2 env_energy_pair(const DevMesh& m, const EnvInfo& e, const Sme
 // predicted correction for alpha = 1, 1/2, 1/4 (a backtracking line search
 // along the prediction: the next alpha is tried only when the previous one
 // did not lower the potential), and keep the first that is lower, else the
-// inertia guess.  The first comparison (alpha = 1) takes one pass over the
-// slots for both potentials.  Every block of a group decides the same way
+// inertia guess.  The potentials are summed over the environment's tet list
+// (each tet once) and its solved vertices; the first comparison (alpha = 1)
+// takes one pass for both.  Every block of a group decides the same way
 // from the same sums.  Returns kStatWarmUsed or 0.
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
 __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
@@ -271,8 +264,8 @@ __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
       }
     }
   };
-  const double2 e01 = env_energy_pair<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc,
-                                                                          s_sum, s_pair, tab);
+  const double2 e01 =
+      env_energy_pair<Real, SReal, MAT, GROUP>(m, e, local, rank, g, sc, s_sum, s_pair, tab);
   const double e0 = e01.x;
   if (e01.y < e0) {  // false on NaN as well
     place(SReal(1));
@@ -282,8 +275,8 @@ __device__ unsigned warm_start_stage(const DevMesh& m, const EnvInfo& e,
   for (int trial = 1; trial < 3; ++trial) {
     place(SReal(1.0 / double(1 << trial)));
     __syncthreads();
-    const double e1 = env_energy<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, local, rank, g, sc, true,
-                                                                     s_sum, s_esum, buf, tab);
+    const double e1 =
+        env_energy<Real, SReal, MAT, GROUP>(m, e, local, rank, g, sc, s_sum, s_esum, buf, tab);
     buf ^= 1;
     if (e1 < e0) return (unsigned)kStatWarmUsed;
   }

@@ -193,16 +193,11 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
       __syncthreads();  // s_total is reused by the next sum
       return total;
     };
-    // incremental potential of the current U
-    auto grid_energy = [&](bool inertia, int slot, bool& ok) -> double {
-      double acc = 0.0;
-      for (int c = 0; c < e.ncolors; ++c) {
-        const ColorInfo ci = m.color[e.cbase + c];
-        for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
-             q += nb * nwarps)
-          acc += energy_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc,
-                                                          inertia, tab);
-      }
+    // incremental potential of the current U: the tets' strain energy (each
+    // tet once, from the mesh's tet list) plus the solved vertices' inertia
+    auto grid_energy = [&](int slot, bool& ok) -> double {
+      double acc = tet_energy<Real, SReal, MAT>(m, e, state, tab, tid, nthreads, false).x;
+      acc += inertia_energy<SReal>(m, e, state, sc, tid, nthreads, false);
       return grid_sum(acc, slot, ok);
     };
     auto place = [&](SReal alpha) {
@@ -217,25 +212,16 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
         }
       }
     };
-    // the potential at the inertia guess (U) and at the full prediction in
-    // one pass (energy_chunk_pair forms the shifted positions exactly as
-    // place(1) stores them, so both sums equal separate passes bit for bit)
+    // the potential at the inertia guess (U; its inertia energy is zero) and
+    // at the full prediction in one pass (tet_energy forms the shifted
+    // positions exactly as place(1) stores them)
     bool ok = true;
     double e0, e1;
     {
-      double a0 = 0.0, a1 = 0.0;
-      for (int c = 0; c < e.ncolors; ++c) {
-        const ColorInfo ci = m.color[e.cbase + c];
-        for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
-             q += nb * nwarps) {
-          const double2 p2 =
-              energy_chunk_pair<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, tab);
-          a0 += p2.x;
-          a1 += p2.y;
-        }
-      }
-      e0 = grid_sum(a0, 0, ok);
-      e1 = ok ? grid_sum(a1, 1, ok) : 0.0;
+      const double2 el = tet_energy<Real, SReal, MAT>(m, e, state, tab, tid, nthreads, true);
+      const double in1 = inertia_energy<SReal>(m, e, state, sc, tid, nthreads, true);
+      e0 = grid_sum(el.x, 0, ok);
+      e1 = ok ? grid_sum(el.y + in1, 1, ok) : 0.0;
     }
     bool used = ok && e1 < e0;  // false on NaN as well
     if (used) {
@@ -249,7 +235,7 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
       bar += nb;
       ok = grid_sync(ctl, bar, lim, &s_ok);
       if (!ok) break;
-      const double et = grid_energy(true, 1 + trial, ok);
+      const double et = grid_energy(1 + trial, ok);
       used = ok && et < e0;
     }
     if (!ok) {
