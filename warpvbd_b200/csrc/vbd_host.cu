@@ -692,7 +692,7 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
 // single-block environment, all block time / resident blocks).  With the
 // learned warm start, job lengths use the high sweep estimate (the maximum
 // of the last eight steps) and the total block time the mean, both plus the
-// cost of its energy checks (1.9 sweeps): its counts vary from step to step,
+// cost of its energy checks (0.7 sweeps): its counts vary from step to step,
 // and an environment whose count jumps while it runs alone on one block sets
 // the step time.  Blocks are listed longest first, which the block scheduler
 // then starts first.
@@ -705,8 +705,8 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
   std::vector<double> d1(n), dC(n), m1(n), mC(n);  // high and mean estimates
   const bool hist = s->env_sweeps.size() == (size_t)n && s->env_sweeps_mean.size() == (size_t)n &&
                     s->env_sweeps_decay.size() == (size_t)n;
-  // the learned warm start's energy checks cost about 1.9 sweeps (measured)
-  const double kw = s->warm ? 1.9 : 0.0;
+  // the learned warm start's energy checks cost about 0.7 sweeps (measured)
+  const double kw = s->warm ? 0.7 : 0.0;
   for (int e = 0; e < n; ++e) {
     const double last = iters ? (double)iters[e] : 1.0;
     double k = last, km = last;
