@@ -233,6 +233,16 @@ int vbd_ws_targets(vbd_solver* s, const float* features, float* targets);
  * step runs), into device [n_vertices][4] (xyz in metres, w = 1 where
  * predicted). */
 int vbd_ws_predict(vbd_solver* s, const float* features, float* predictions);
+/* The incremental potential the warm start's check evaluates, per
+ * environment, at `positions` (host float64 [n_vertices][3], caller order) for
+ * a step of length dt from the current state: the strain energy of every tet
+ * with a solved vertex plus, over the solved vertices,
+ * m/(2 dt^2) |x - (x0 + dt v + dt^2 g)|^2 (vbd_solver.py:15-146 descend its
+ * gradient; the SNH energy differs from the reference's by a constant per
+ * tet).  potential_out: host float64 [n_env].  Allocates a scratch state on
+ * first use. */
+int vbd_incremental_potential(vbd_solver* s, double dt, const double* positions,
+                              double* potential_out);
 /* Per-environment status bits of the last step: 1 non-finite, 2 guarded
  * step taken, 4 max_iter reached, 16 started from the learned prediction. */
 int vbd_get_env_status(vbd_solver* s, uint32_t* status_out);

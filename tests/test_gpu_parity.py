@@ -252,6 +252,37 @@ def test_step_timeline():
     assert len(traced.timeline()["env"]) == 0
 
 
+@pytest.mark.parametrize("precision,tol", [("mixed", 1e-4), ("fp64", 1e-9)])
+def test_incremental_potential_matches_oracle(precision, tol):
+    """The potential the learned warm start compares (each tet's strain energy
+    once from the tet list, plus the solved vertices' inertia energy), as
+    differences between two candidate states, against the FP64 oracle's
+    incremental potential: the two differ only by constants (the SNH
+    energy's constant per tet and the inertia form's x-independent terms).
+    Relative tolerance on the difference: 1e-4 with fp32 strain energies,
+    1e-9 in FP64."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(3, seed=7)
+    b = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, precision=precision)
+    for _ in range(3):
+        b.step(1e-3)
+    x, v = b.positions(), b.velocities()
+    act = np.concatenate([e.active for e in envs])[:, None]
+    rng = np.random.default_rng(1)
+    xa = x + 2e-4 * rng.normal(size=x.shape) * act
+    xb = x + 2e-4 * rng.normal(size=x.shape) * act
+    ea, eb = b.incremental_potential(xa), b.incremental_potential(xb)
+    for e, env in enumerate(envs):
+        o = oracle.OracleSolver(**env.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7,
+                                max_iter=1000)
+        sl = b.env_slice(e)
+        o.set_state(x[sl], v[sl])
+        d_o = o.incremental_potential(xa[sl], 1e-3) - o.incremental_potential(xb[sl], 1e-3)
+        d_k = ea[e] - eb[e]
+        print(f"{precision} env {e}: difference {d_k:.9e} vs oracle {d_o:.9e}")
+        assert abs(d_k - d_o) <= tol * abs(d_o), (e, d_k, d_o)
+
+
 def test_downloads_into_caller_arrays():
     """positions(out=...) / DeviceArray.numpy(out=...) fill a caller array
     (e.g. page-locked) with exactly what a fresh download returns."""

@@ -84,6 +84,7 @@ SIGNATURES = {
     "vbd_get_trace": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int,
                                      _ip]),
     "vbd_ws_vertex_rows": (ctypes.c_int, [_vp, _i]),
+    "vbd_incremental_potential": (ctypes.c_int, [_vp, ctypes.c_double, _d, _d]),
     "vbd_step": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip]),
     "vbd_step_batched": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _d,
                                         ctypes.c_int, _ip]),

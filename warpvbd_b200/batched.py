@@ -193,6 +193,18 @@ class BatchedVBDSolver:
     def ws_features(self, dt, out=None):
         return _ws_features(self._h, self.n_vertices, dt, out)
 
+    def incremental_potential(self, positions, dt=1e-3):
+        """Per-environment incremental potential at `positions` (caller order)
+        for a step of length dt from the current state: the strain energy of
+        every tet with a solved vertex plus the solved vertices' inertia
+        energy, as the learned warm start's check evaluates it."""
+        x = _lib.f64(positions, (self.n_vertices, 3))
+        out = np.zeros(self.n_env)
+        _lib.check(_lib.load().vbd_incremental_potential(self._h, float(dt), _lib.ptr(x, "d"),
+                                                         _lib.ptr(out, "d")),
+                   "vbd_incremental_potential")
+        return out
+
     def ws_vertex_rows(self):
         """Row of every vertex (caller order) in the feature, target and
         prediction arrays."""

@@ -478,6 +478,9 @@ struct vbd_solver {
   DevBuf<ushort4> d_rec_idx16;
   DevBuf<int4> d_tet_slot;
   DevBuf<int> d_tet_owner;
+  // vbd_incremental_potential: candidate state (Real4) and per-env results
+  DevBuf<unsigned char> d_xeval;
+  DevBuf<double> d_pot;
   DevBuf<unsigned char> d_rec_tab;
   int fmt = kFmtIdx32;
   DevBuf<int> d_valence, d_map, d_iters;
@@ -601,6 +604,8 @@ void free_solver(vbd_solver* s) {
   s->d_rec_idx16.release();
   s->d_tet_slot.release();
   s->d_tet_owner.release();
+  s->d_xeval.release();
+  s->d_pot.release();
   s->d_rec_tab.release();
   s->d_valence.release();
   s->d_map.release();
@@ -1688,6 +1693,36 @@ int vbd_ws_features(vbd_solver* s, double dt, float* features) {
   CUDA_TRY(launch_ws_features(s->prec, s->tpv, s->mesh(), (int)s->L.chunk.size(), dt, s->g,
                               s->ws_history ? 1 : 0, s->d_wpack.p, features, s->stream));
   CUDA_TRY(cudaStreamSynchronize(s->stream));
+  return VBD_OK;
+}
+
+int vbd_incremental_potential(vbd_solver* s, double dt, const double* positions,
+                              double* potential_out) {
+  if (!s || !positions || !potential_out) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(VBD_ERR_INVALID_ARG, "dt must be > 0");
+  DeviceGuard dg(s->device);
+  cudaStream_t st = s->stream;
+  if (s->pending) {
+    const int rc = finish(s, nullptr);
+    if (rc < 0) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (!s->d_xeval.p) {
+    CUDA_TRY(s->d_xeval.alloc(s->real4_bytes * (size_t)s->V));
+    CUDA_TRY(cudaMemset(s->d_xeval.p, 0, s->real4_bytes * (size_t)s->V));
+  }
+  if (!s->d_pot.p) CUDA_TRY(s->d_pot.alloc((size_t)s->n_env));
+  StepParams p{};
+  p.dt = dt;
+  p.kd = s->kd;
+  for (int i = 0; i < 3; ++i) p.g[i] = s->g[i];
+  CUDA_TRY(cudaMemcpyAsync(s->d_io.p, positions, sizeof(double) * 3 * (size_t)s->V,
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(launch_scatter(s->state64, s->d_X.p, s->d_map.p, s->d_io.p, s->d_xeval.p, s->V, st));
+  CUDA_TRY(launch_potential(s->prec, s->material, s->mesh(), p, s->d_xeval.p, s->d_pot.p, st));
+  CUDA_TRY(cudaMemcpyAsync(potential_out, s->d_pot.p, sizeof(double) * s->n_env,
+                           cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
   return VBD_OK;
 }
 

@@ -602,10 +602,72 @@ struct ColorLaunch {
   }
 };
 
+// Incremental potential of every environment at a candidate state `x`
+// (displacements, renumbered), for a step of length dt from the current state
+// (u, vel): the same tet-list strain energy and inertia energy the learned
+// warm start compares, with the inertia target formed as begin_vertex forms
+// it (not written back).  One block per environment.
+template <typename Real, typename SReal, int MAT>
+__global__ void __launch_bounds__(256) potential_kernel(DevMesh m, StepParams p,
+                                                        const real4<SReal>* __restrict__ x,
+                                                        double* __restrict__ out) {
+  using S4 = real4<SReal>;
+  using R4 = real4<Real>;
+  const EnvInfo e = m.env[blockIdx.x];
+  const StepConst sc = make_const(p);
+  const GlobalState<SReal> st{const_cast<S4*>(x) + e.vbase};  // read only
+  const R4* tab = reinterpret_cast<const R4*>(m.rec_tab) + 3 * (size_t)e.rbase;
+  double acc = tet_energy<Real, SReal, MAT>(m, e, st, tab, threadIdx.x, blockDim.x, false).x;
+  const S4* U = reinterpret_cast<const S4*>(m.u) + e.vbase;
+  const S4* V = reinterpret_cast<const S4*>(m.vel) + e.vbase;
+  const S4* UT = reinterpret_cast<const S4*>(m.ut) + e.vbase;
+  for (int i = threadIdx.x; i < e.nsolved; i += blockDim.x) {
+    const S4 u0 = U[i], v0 = V[i], xi = x[e.vbase + i];
+    const SReal dt = SReal(sc.dt), dt2 = SReal(sc.dt2);
+    const SReal tx = u0.x + v0.x * dt + SReal(sc.g[0]) * dt2;
+    const SReal ty = u0.y + v0.y * dt + SReal(sc.g[1]) * dt2;
+    const SReal tz = u0.z + v0.z * dt + SReal(sc.g[2]) * dt2;
+    const double dx = double(xi.x - tx), dy = double(xi.y - ty), dz = double(xi.z - tz);
+    acc += 0.5 * double(UT[i].w) * sc.inv_dt2 * (dx * dx + dy * dy + dz * dz);
+  }
+  __shared__ double s_part[8];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s_part[w];
+    out[blockIdx.x] = v;
+  }
+}
+
+struct PotentialLaunch {
+  const DevMesh& m;
+  const StepParams& p;
+  const void* x;
+  double* out;
+  cudaStream_t s;
+  template <typename Real, typename SReal, int TPV, int MAT, int FMT>
+  cudaError_t run() {
+    if (TPV != 4 || FMT != kFmtIdx32) return cudaSuccess;  // one instantiation per precision
+    potential_kernel<Real, SReal, MAT><<<m.n_env, 256, 0, s>>>(
+        m, p, static_cast<const real4<SReal>*>(x), out);
+    return cudaGetLastError();
+  }
+};
+
 inline int nblk(int n, int t) { return (n + t - 1) / t; }
 }  // namespace
 
 int env_kernel_max_smem() { return kMaxSmem; }
+
+cudaError_t launch_potential(int prec, int material, const DevMesh& m, const StepParams& p,
+                             const void* x, double* out, cudaStream_t s) {
+  if (m.n_env <= 0) return cudaSuccess;
+  PotentialLaunch f{m, p, x, out, s};
+  return dispatch(prec, material, kFmtIdx32, 4, f);
+}
 
 cudaError_t launch_env_step(int prec, int material, int tpv, int threads, const DevMesh& m,
                             const StepParams& p, const double* tol_env, const int4* work,

@@ -43,6 +43,11 @@ cudaError_t launch_gather(bool state64, const double* offset, const int* new_of_
                           const void* state, double* out, int n, cudaStream_t s);
 cudaError_t launch_scatter(bool state64, const double* offset, const int* new_of_old,
                            const double* in, void* state, int n, cudaStream_t s);
+// Incremental potential of every environment at the renumbered displacements
+// x (Real4 in the state precision) for a step with the parameters p from the
+// current state; out: device double [n_env].
+cudaError_t launch_potential(int prec, int material, const DevMesh& m, const StepParams& p,
+                             const void* x, double* out, cudaStream_t s);
 // Sets the xyz of every state vector to zero, keeping w.
 cudaError_t launch_zero_xyz(bool state64, void* state, int n, cudaStream_t s);
 

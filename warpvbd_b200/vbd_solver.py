@@ -280,6 +280,18 @@ class VBDSolver:
         E, nu = self.youngs_modulus, self.poissons_ratio
         return E / (2.0 * (1.0 + nu)), (E * nu) / ((1.0 + nu) * (1.0 - 2.0 * nu))
 
+    def incremental_potential(self, positions, dt=1e-3):
+        """Incremental potential at `positions` for a step of length dt from
+        the current state (strain energy of the tets with a solved vertex plus
+        the solved vertices' inertia energy; no counterpart in the reference,
+        whose step descends its gradient)."""
+        x = _lib.f64(positions, (self.n_vertices, 3))
+        out = np.zeros(1)
+        _lib.check(_lib.load().vbd_incremental_potential(self._h, float(dt), _lib.ptr(x, "d"),
+                                                         _lib.ptr(out, "d")),
+                   "vbd_incremental_potential")
+        return float(out[0])
+
     def info(self):
         L = _lib.load()
         inf = _lib.VBDInfo()
