@@ -84,6 +84,14 @@ __global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunk
   const S4* U = reinterpret_cast<const S4*>(m.u);
   const S4* VEL = reinterpret_cast<const S4*>(m.vel);
   const ChunkInfo ch = m.chunk[q];
+  // the chunk's slot indices up to the prefetch depth first, as the sweep does
+  using RS = RawSlot<FMT>;
+  constexpr int PF = Prefetch<TPV>::steps;
+  const size_t base = (size_t)ch.block * 32 + lane;
+  typename RS::type sl[PF];
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps) sl[s] = RS::load(m, base + (size_t)s * 32);
   int k = 0;
   S4 uo, vo;
   uo.x = uo.y = uo.z = uo.w = SReal(0);
@@ -96,24 +104,25 @@ __global__ void __launch_bounds__(256) ws_features_kernel(DevMesh m, int n_chunk
   float su[3] = {0.f, 0.f, 0.f}, sv[3] = {0.f, 0.f, 0.f};
   const float ux = float(uo.x), uy = float(uo.y), uz = float(uo.z);
   const float vx = float(vo.x), vy = float(vo.y), vz = float(vo.z);
-  const size_t base = (size_t)ch.block * 32 + lane;
-  for (int s = 0; s < ch.steps; ++s) {
-    if (s * TPV + sub < k) {
-      const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
-      const int nb[3] = {id.x, id.y, id.z};
+  auto visit = [&](const int4& id) {
+    const int nb[3] = {id.x, id.y, id.z};
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        const float4 a = __ldg(pa + vbase + nb[j]);
-        const float2 b = __ldg(pb + vbase + nb[j]);
-        su[0] += a.x - ux;
-        su[1] += a.y - uy;
-        su[2] += a.z - uz;
-        sv[0] += a.w - vx;
-        sv[1] += b.x - vy;
-        sv[2] += b.y - vz;
-      }
+    for (int j = 0; j < 3; ++j) {
+      const float4 a = __ldg(pa + vbase + nb[j]);
+      const float2 b = __ldg(pb + vbase + nb[j]);
+      su[0] += a.x - ux;
+      su[1] += a.y - uy;
+      su[2] += a.z - uz;
+      sv[0] += a.w - vx;
+      sv[1] += b.x - vy;
+      sv[2] += b.y - vz;
     }
-  }
+  };
+#pragma unroll
+  for (int s = 0; s < PF; ++s)
+    if (s < ch.steps && s * TPV + sub < k) visit(RS::unpack(sl[s]));
+  for (int s = PF; s < ch.steps; ++s)
+    if (s * TPV + sub < k) visit(load_slot<FMT>(m, base + (size_t)s * 32));
 #pragma unroll
   for (int off = TPV / 2; off > 0; off >>= 1) {
 #pragma unroll
