@@ -304,3 +304,39 @@ def test_downloads_into_caller_arrays():
     assert np.array_equal(x, v.old_positions.numpy())
     with pytest.raises(ValueError):
         v.old_positions.numpy(out=np.empty((3, 3)))
+
+
+def test_random_voxel_shapes_match_oracle():
+    """Property test: random voxel shapes (up to 6 x 4 x 4, the x = 0 face
+    fixed), random stiffness; the block-mode solver against the FP64 oracle
+    for 20 steps, same per-vertex tolerance as the cantilever."""
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as st
+
+    from warpvbd_b200 import VBDSolver, mesh
+
+    @settings(max_examples=8, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+    @given(st.integers(2, 6), st.integers(1, 4), st.integers(1, 4),
+           st.lists(st.booleans(), min_size=96, max_size=96), st.floats(1e5, 1e6))
+    def check(nx, ny, nz, bits, youngs):
+        vox = np.array(bits[:nx * ny * nz], bool).reshape(nx, ny, nz)
+        vox[0] = True  # the fixed face and something attached to it
+        vox[:, 0, 0] = True
+        h = 0.02
+        X, hexes = mesh.voxel2hex(vox, h, h, h)
+        T = np.asarray(mesh.hex2tets(hexes), np.int32).reshape(-1, 4)
+        n_t = T.shape[0]
+        kw = dict(initial_positions=X, elements=T, densities=np.full(n_t, 1000.0),
+                  youngs_modulus=np.full(n_t, youngs), poissons_ratio=np.full(n_t, 0.4),
+                  active_mask=X[:, 0] > 1e-9)
+        gpu = VBDSolver(**kw, damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000, mode="block")
+        orc = oracle.OracleSolver(**kw, damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000,
+                                  guarded=True)
+        D = _diag(X)
+        for _ in range(20):
+            xg = gpu.step(gpu.old_positions, 1e-3).numpy()
+            xo = orc.step(None, 1e-3)
+            assert np.abs(xg - xo).max() / D < POS_TOL
+            assert abs(gpu.last_iterations - orc.last_iterations) <= 2
+
+    check()
