@@ -247,12 +247,12 @@ def run_reference(args, envs, desc, batched):
     if rank != 0:
         return
     sample = cpu_sample(envs, batched)
-    v, k, n, el = oracle_rate(sample, args.reference_budget_s, args.steps, warmup=0)
+    v, k, n, el = oracle_rate(sample, args.reference_budget_s, args.steps, warmup=args.warmup)
     what = (f"{len(sample)} of the {len(envs)} environments concatenated into one mesh "
             "(the reference's batching, one global convergence test)") if batched else \
         "the whole mesh"
     line = {"impl": "reference", "metric": "sim-s/wall-s", "value": v, "unit": "sim-s/wall-s",
-            "n_gpus": args.gpus, "steps": k, "warmup": 0, "ms_per_step": 1e3 * el / k,
+            "n_gpus": args.gpus, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * el / k,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": desc, "dt": DT, "tol": TOL, "max_iter": MAX_ITER},
@@ -368,18 +368,21 @@ def run_ours(args, envs, desc, batched):
     # from page-locked host memory and downloads the new ones into it
     n_vertices = sum(e.n_vertices for e in envs)
     xh = torch.empty((n_vertices, 3), dtype=torch.float64, pin_memory=True).numpy()
+    # (three untimed round trips first, as for the device-timed steps)
     if batched:
         sol.positions(out=xh)
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
+        for k in range(3 + args.e2e_steps):
+            if k == 3:
+                t0 = time.perf_counter()
             sol.set_state(positions=xh)
             sol.step(DT)
             sol.positions(out=xh)
         e2e_s = time.perf_counter() - t0
     else:
         sol.old_positions.numpy(out=xh)
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
+        for k in range(3 + args.e2e_steps):
+            if k == 3:
+                t0 = time.perf_counter()
             sol.step(xh, DT).numpy(out=xh)
         e2e_s = time.perf_counter() - t0
     e2e = world * n_env * args.e2e_steps * DT / e2e_s
@@ -536,7 +539,7 @@ def main():
     ap.add_argument("--workload", default="batch256")
     ap.add_argument("--mode", default="auto",
                     choices=["auto", "block", "graph", "hostloop", "persist"])
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--secondary-steps", type=int, default=30)
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
