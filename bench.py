@@ -404,7 +404,9 @@ def run_ours(args, envs, desc, batched):
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     kernel = {"block": "env_step_kernel", "persist": "persist_kernel"}.get(mode, "color_kernel")
-    tps = profile_traffic_per_slot(kernel, args.workload)
+    # the capture of the same setting (warm-started or plain), else the other
+    tps = (profile_traffic_per_slot(kernel, args.workload + ".warm") if warm is not None
+           else None) or profile_traffic_per_slot(kernel, args.workload)
     traffic = None if tps is None else tps * float((passes * slots[None, :]).sum()) / args.steps
     launches = int(np.sum(detail["launches"]))  # counted by the library, per step
     line = {"metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s",
