@@ -57,9 +57,10 @@ def slot_grad_hess(material, X4, x4, a, mu, lam):
     return g, H
 
 
-def slot_energy(material, X4, x4, a, mu, lam):
+def slot_psi(material, X4, x4, a, mu, lam):
     """Strain energy of one tet seen from its vertex a, kernel closed form
-    (slot_energy in warpvbd_b200/csrc/vbd_device.cuh, before the slot weight):
+    (slot_psi in warpvbd_b200/csrc/vbd_device.cuh; the kernel evaluates it from
+    each tet's owner slot, its solved vertex of lowest id):
     SNH  p0/2 (Ic - 3 - ln(1 + (Ic - 3)/4)) + p1/2 (J - 1 - 3/4 p0/p1)^2, i.e.
          the reference's mu'/2 (Ic - 3) - mu'/2 ln(Ic + 1) + lambda'/2 (J - alpha)^2
          up to the constant mu'/2 ln 4, with J - 1 and Ic - 3 from G = F - I;

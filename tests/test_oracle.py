@@ -228,9 +228,10 @@ def test_numpy_twin_single_sweep():
 @pytest.mark.parametrize("material,code", [("snh", oracle.SNH), ("stvk", oracle.STVK)])
 def test_kernel_energy_matches_oracle_up_to_a_constant(material, code):
     """The learned warm start accepts a prediction by comparing potentials, so
-    the kernel's per-slot energy (restated in tests/kernel_math.py) must
-    differ from the oracle's tet energy only by a constant: energy
-    differences between deformations agree, from every vertex's slot."""
+    the kernel's tet energy (restated in tests/kernel_math.py) must differ
+    from the oracle's only by a constant: energy differences between
+    deformations agree, seen from every vertex of the tet (the kernel uses
+    one, the tet's owner)."""
     rng = np.random.default_rng(7)
     mu, lam = 3.4e5, 3.1e6
     for _ in range(20):
@@ -241,6 +242,6 @@ def test_kernel_energy_matches_oracle_up_to_a_constant(material, code):
         d_or = (oracle.tet_energy(code, x1, inv, mu, lam, vol)
                 - oracle.tet_energy(code, x0, inv, mu, lam, vol))
         for a in range(4):
-            d_k = (kernel_math.slot_energy(material, X4, x1, a, mu, lam)
-                   - kernel_math.slot_energy(material, X4, x0, a, mu, lam))
+            d_k = (kernel_math.slot_psi(material, X4, x1, a, mu, lam)
+                   - kernel_math.slot_psi(material, X4, x0, a, mu, lam))
             assert abs(d_k - d_or) <= 1e-9 * max(1.0, abs(d_or)), (a, d_k, d_or)
