@@ -49,6 +49,8 @@ typedef struct vbd_solver vbd_solver;
 #define VBD_ERR_TIMEOUT (-6)         /* a bounded device-side wait gave up */
 #define VBD_ERR_NO_DEVICE (-7)
 #define VBD_ERR_UNSUPPORTED (-8)     /* e.g. an environment too large for block mode */
+#define VBD_ERR_BOUNDS (-9)          /* bounds-checked build (libvbd_b200_check.so): a slot
+                                        index out of range; the access was skipped */
 
 /* ---- flags --------------------------------------------------------------- */
 #define VBD_MATERIAL_SNH 0x0  /* Stable Neo-Hookean, vbd_solver.py:107-124 */

@@ -11,7 +11,9 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libvbd_b200.so")
+# WARPVBD_B200_LIB selects another build of the library, e.g. the
+# bounds-checked libvbd_b200_check.so (`make -C warpvbd_b200/csrc check`)
+LIB_PATH = os.environ.get("WARPVBD_B200_LIB") or os.path.join(_HERE, "libvbd_b200.so")
 CSRC = os.path.join(_HERE, "csrc")
 
 # status codes
@@ -25,6 +27,7 @@ ERR_NONFINITE = -5
 ERR_TIMEOUT = -6
 ERR_NO_DEVICE = -7
 ERR_UNSUPPORTED = -8
+ERR_BOUNDS = -9
 
 # flags
 MATERIAL_SNH = 0x0

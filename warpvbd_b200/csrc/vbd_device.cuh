@@ -284,6 +284,14 @@ struct RawSlot<kFmtIdx32> {
   static __device__ __forceinline__ int4 unpack(const int4& s) { return s; }
 };
 
+// Bounds-checked build (make check -> libvbd_b200_check.so): every slot's
+// neighbour and record ids, and the vertex's own id, are checked against its
+// environment before use; an id out of range sets kStatBounds (the step then
+// fails with VBD_ERR_BOUNDS) and the access is skipped.
+#ifndef VBD_CHECK_BOUNDS
+#define VBD_CHECK_BOUNDS 0
+#endif
+
 // Slot steps of a chunk whose indices are loaded up front: enough for the
 // reference's 20 incident tets per vertex (MAX_ELEMENTS_PER_VERTEX); longer
 // chunks stream the rest.
@@ -320,11 +328,20 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
 #pragma unroll
   for (int s = 0; s < PF; ++s)
     if (s < ch.steps) sl[s] = RS::load(m, base + (size_t)s * 32);
+#if VBD_CHECK_BOUNDS
+  // the vertex itself: a lane with an id out of range does no work, but stays
+  // in the warp for the shuffles below
+  const EnvInfo eb = m.env[m.chunk_owner[q].y];
+  const bool vbad = valid && (lv < 0 || lv >= eb.nsolved);
+  if (vbad) stat |= kStatBounds;
+#else
+  constexpr bool vbad = false;
+#endif
   int k = 0;
   S4 uo, tt;
   uo.x = uo.y = uo.z = uo.w = SReal(0);
   tt = uo;
-  if (valid) {
+  if (valid && !vbad) {
     k = __ldg(m.valence + gv);
     uo = st.load(lv);
     // ut / up are written in this launch by another block of a group: read
@@ -336,6 +353,13 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
   // the environment's record table: shared memory (staged by the caller) or
   // global memory, read through the same generic pointer
   auto visit = [&](const int4& id) {
+#if VBD_CHECK_BOUNDS
+    if ((unsigned)id.x >= (unsigned)eb.nv || (unsigned)id.y >= (unsigned)eb.nv ||
+        (unsigned)id.z >= (unsigned)eb.nv || (unsigned)id.w >= (unsigned)eb.nrec) {
+      stat |= kStatBounds;
+      return;
+    }
+#endif
     const R4* t = tab + 3 * (size_t)id.w;
     const R4 q0 = t[0];
     const R4 q1 = t[1];
@@ -361,7 +385,7 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
 #pragma unroll
     for (int i = 0; i < 6; ++i) h[i] += __shfl_xor_sync(0xffffffffu, h[i], off);
   }
-  if (valid && sub == 0) {
+  if (valid && !vbad && sub == 0) {
     const Real mdt2 = Real(tt.w * SReal(sc.inv_dt2));
     Real G[3], H[6];
     G[0] = g[0] + mdt2 * Real(uo.x - tt.x);

@@ -1142,6 +1142,7 @@ int status_from_bits(const vbd_solver* s, const unsigned* st) {
     if ((b & kStatGuard) && (s->flags & VBD_STRICT_SPD))
       return fail(VBD_ERR_NONFINITE, "3x3 vertex block not positive definite");
     if (b & kStatTimeout) return fail(VBD_ERR_TIMEOUT, "device-side wait timed out");
+    if (b & kStatBounds) return fail(VBD_ERR_BOUNDS, "slot index out of range (checked build)");
     if (b & kStatIterCap) rc = VBD_NOT_CONVERGED;
   }
   return rc;

@@ -39,6 +39,7 @@ enum StatusBits : unsigned {
   kStatIterCap = 4u,    // max_iter reached without convergence
   kStatTimeout = 8u,
   kStatWarmUsed = 16u,  // the step started from the learned prediction
+  kStatBounds = 32u,    // bounds-checked build: a slot index out of range (access skipped)
 };
 
 struct EnvInfo {
