@@ -11,9 +11,13 @@
 //             active vertices start from ut                      | barrier
 //   sweep     for each colour: warps take the colour's chunks grid-stride
 //             and update their vertices (process_chunk); colours are
-//             separated by a grid barrier, except that a run of colours
-//             small enough for one block (<= warps per block chunks) is
-//             done by block 0 alone with __syncthreads between them
+//             separated by a grid barrier, except inside a run of small
+//             colours (at most kSmallBlocks blocks' worth of chunks, e.g.
+//             the 107-vertex colours of a voxel cantilever): those are
+//             done by the first S blocks only (S = blocks the largest small
+//             colour needs), which meet at a barrier among themselves
+//             (__syncthreads when S = 1) while the others go on to the next
+//             grid barrier
 //             end of sweep: block max of |dx_x+dx_y+dx_z| -> atomicMax on
 //             a rotating slot; the grid barrier; every block reads the slot
 //             and takes the same stop decision
@@ -86,19 +90,21 @@ __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
   return v;
 }
 
-// Grid barrier number target / gridDim.x.  Returns false if the launch is
-// aborting (this block's wait expired, or another block's did).
-__device__ __forceinline__ bool grid_sync(PersistCtl* ctl, unsigned long long target,
-                                          const PersistLimits& lim, int* s_ok) {
+// Barrier on `counter` among the blocks that use it: passed when the counter
+// reaches `target` (the number of barriers so far x the participants).
+// Returns false if the launch is aborting (this block's wait expired, or
+// another block's did).
+__device__ __forceinline__ bool counter_sync(PersistCtl* ctl, unsigned long long* counter,
+                                             unsigned long long target,
+                                             const PersistLimits& lim, int* s_ok) {
   __syncthreads();
-  if (gridDim.x == 1) return true;  // one block: __syncthreads is the barrier
   if (threadIdx.x == 0) {
     int ok = 1;
     __threadfence();
-    red_release_add_u64(&ctl->arrivals, 1ull);
+    red_release_add_u64(counter, 1ull);
     const unsigned long long t0 = globaltimer_ns();
     for (long long n = 0;; ++n) {
-      if (ld_acquire_u64(&ctl->arrivals) >= target) break;
+      if (ld_acquire_u64(counter) >= target) break;
       const bool expired = n >= lim.max_polls ||
                            ((n & 255) == 255 && globaltimer_ns() - t0 > lim.max_wait_ns);
       if (expired || ld_relaxed_u32(&ctl->abort) != 0u) {
@@ -116,6 +122,20 @@ __device__ __forceinline__ bool grid_sync(PersistCtl* ctl, unsigned long long ta
   __syncthreads();
   return *s_ok != 0;
 }
+
+// Grid barrier number target / gridDim.x.
+__device__ __forceinline__ bool grid_sync(PersistCtl* ctl, unsigned long long target,
+                                          const PersistLimits& lim, int* s_ok) {
+  if (gridDim.x == 1) {  // one block: __syncthreads is the barrier
+    __syncthreads();
+    return true;
+  }
+  return counter_sync(ctl, &ctl->arrivals, target, lim, s_ok);
+}
+
+// A colour of at most kSmallBlocks x (warps per block) chunks is "small": it
+// runs on the first few blocks only.
+constexpr int kSmallBlocks = 8;
 
 template <typename Real, typename SReal, int TPV, int MAT, int FMT>
 __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
@@ -249,29 +269,43 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
       VBD_GRID_SYNC();
     }
   }
+  // small colours run on the first nsb blocks: as many as the largest of
+  // them needs for one chunk per warp
+  auto is_small = [&](int nch) { return nb > 1 && nch <= kSmallBlocks * nwarps; };
+  int nsb = 1;
+  for (int c = 0; c < e.ncolors; ++c) {
+    const int nch = m.color[e.cbase + c].chunk_end - m.color[e.cbase + c].chunk_begin;
+    if (is_small(nch)) nsb = max(nsb, (nch + nwarps - 1) / nwarps);
+  }
+  nsb = min(nsb, nb);
+  unsigned long long sub_bar = 0ull;  // arrivals that complete the next small-colour barrier
   int it = 0;
   bool conv = false, nan = false;
   for (;;) {
     unsigned long long cmax = 0ull;
     for (int c = 0; c < e.ncolors; ++c) {
       const ColorInfo ci = m.color[e.cbase + c];
-      const int nch = ci.chunk_end - ci.chunk_begin;
-      const bool local = nb > 1 && nch <= nwarps;
-      if (local) {
-        if (blockIdx.x == 0 && warp < nch)
-          process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, ci.chunk_begin + warp, lane,
-                                                    state, sc, cmax, stat, tab);
-      } else {
+      const bool small = is_small(ci.chunk_end - ci.chunk_begin);
+      const int span = small ? nsb : nb;  // blocks that take this colour
+      if (blockIdx.x < span)
         for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
-             q += nb * nwarps)
+             q += span * nwarps)
           process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, cmax,
                                                     stat, tab);
-      }
       if (c + 1 == e.ncolors) break;
       const ColorInfo cn = m.color[e.cbase + c + 1];
-      const bool next_local = nb > 1 && (cn.chunk_end - cn.chunk_begin) <= nwarps;
-      if (local && next_local) {
-        __syncthreads();  // block 0 did both colours; its writes are block-visible
+      if (small && is_small(cn.chunk_end - cn.chunk_begin)) {
+        // both colours ran on the small-colour blocks only: they meet among
+        // themselves (block 0 alone: its writes are block-visible)
+        if (nsb == 1) {
+          __syncthreads();
+        } else if (blockIdx.x < nsb) {
+          sub_bar += nsb;
+          if (!counter_sync(ctl, &ctl->sub_arrivals, sub_bar, lim, &s_ok)) {
+            if (threadIdx.x == 0) atomicOr(m.status, kStatTimeout);
+            return;
+          }
+        }
       } else {
         VBD_GRID_SYNC();
       }

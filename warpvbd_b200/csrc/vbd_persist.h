@@ -10,11 +10,11 @@ namespace vbd {
 // Device-side control of one persistent step; zeroed by launch_persist
 // before every launch.
 struct PersistCtl {
-  unsigned long long arrivals;  // grid-barrier arrivals in this step
-  unsigned long long conv[3];   // per-sweep max |dx_x+dx_y+dx_z| bits, slot = sweep % 3
-  unsigned status;              // status bits (kStat*) of every block
-  unsigned abort;               // set when a barrier wait expired
-  unsigned pad[2];
+  unsigned long long arrivals;      // grid-barrier arrivals in this step
+  unsigned long long sub_arrivals;  // arrivals at the barriers among the small-colour blocks
+  unsigned long long conv[3];       // per-sweep max |dx_x+dx_y+dx_z| bits, slot = sweep % 3
+  unsigned status;                  // status bits (kStat*) of every block
+  unsigned abort;                   // set when a barrier wait expired
 };
 
 // Bounds of every grid-barrier wait.
