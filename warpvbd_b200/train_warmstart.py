@@ -1,6 +1,6 @@
 """Train the warm-start network on the GPU and save it.
 
-    python -m warpvbd_b200.train_warmstart [--out PATH] [--seed S] [--epochs E]
+    python -m warpvbd_b200.train_warmstart [--out PATH] [--seed S] [--epochs E] [--lr LR]
 
 Generates ~2M samples from seeded plain-VBD rollouts (cantilever and
 mass-spring environments, E log-uniform in [1e5, 1e7] Pa, nu in [0.30, 0.48],
@@ -25,15 +25,20 @@ def main():
     ap.add_argument("--envs", type=int, default=24)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--every", type=int, default=5)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--batch", type=int, default=4096, help="minibatch size")
+    ap.add_argument("--fine", action="store_true",
+                    help="include 1 m cantilevers of 40 and 80 voxels in the rollouts")
     args = ap.parse_args()
     import torch
     t0 = time.perf_counter()
     X, Y = ws.rollout_dataset(seed=args.seed, n_batches=args.batches,
                               envs_per_batch=args.envs, steps=args.steps,
-                              record_every=args.every)
+                              record_every=args.every, fine=args.fine)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    model, info = ws.train_warmstart(X, Y, epochs=args.epochs, seed=args.seed)
+    model, info = ws.train_warmstart(X, Y, epochs=args.epochs, batch=args.batch, lr=args.lr,
+                                     seed=args.seed)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     ws.save(args.out, model, {"loss": info["loss"], "r2": info["r2"],

@@ -146,15 +146,21 @@ class MLPTrainer:
         return self.P.detach().cpu().numpy().copy()
 
 
-def training_envs(seed, n_env):
+def training_envs(seed, n_env, fine=False):
     """Seeded cantilever and mass-spring environments with random materials
-    (E log-uniform in [1e5, 1e7] Pa, nu uniform in [0.30, 0.48])."""
+    (E log-uniform in [1e5, 1e7] Pa, nu uniform in [0.30, 0.48]).  Cantilevers
+    have 5 cm voxels (10-30 voxels long); with `fine`, every other one is a
+    1 m beam of 40 or 80 voxels (2.5 / 1.25 cm) instead, so that beams of the
+    benchmark's resolutions are in the data too."""
     rng = np.random.default_rng(seed)
     envs = []
     for i in range(n_env):
         E = float(np.exp(rng.uniform(np.log(1e5), np.log(1e7))))
         nu = float(rng.uniform(0.30, 0.48))
-        if i % 3 == 0:
+        if i % 3 == 0 and fine and i % 6 == 0:
+            n = int(rng.choice([40, 80]))
+            envs.append(scenes.cantilever(n, youngs=E, poisson=nu))
+        elif i % 3 == 0:
             n = int(rng.choice([10, 20, 30]))
             envs.append(scenes.cantilever(n, max(1, n // 10), max(1, n // 10), length=n * 0.01 * 5,
                                           youngs=E, poisson=nu))
@@ -165,7 +171,8 @@ def training_envs(seed, n_env):
 
 
 def rollout_dataset(seed=1, n_batches=6, envs_per_batch=24, steps=100, record_every=5,
-                    dt=1e-3, tol=1e-7, max_iter=1000, velocity_noise=0.1, device="cuda"):
+                    dt=1e-3, tol=1e-7, max_iter=1000, velocity_noise=0.1, device="cuda",
+                    fine=False):
     """Plain-VBD rollouts on the GPU: every `record_every` steps the features
     at the step start and the correction the step converged to.  Each batch
     has its own random gravity direction; every active vertex starts with
@@ -176,7 +183,7 @@ def rollout_dataset(seed=1, n_batches=6, envs_per_batch=24, steps=100, record_ev
     rng = np.random.default_rng(seed)
     Xs, Ys = [], []
     for b in range(n_batches):
-        envs = training_envs(int(rng.integers(1 << 31)), envs_per_batch)
+        envs = training_envs(int(rng.integers(1 << 31)), envs_per_batch, fine=fine)
         # batch 0 falls along -z; the others along a random direction
         d = np.array([0.0, 0.0, -1.0]) if b == 0 else rng.normal(size=3)
         g = 9.81 * d / np.linalg.norm(d)
