@@ -164,6 +164,16 @@ int vbd_reset(vbd_solver* s);
 int vbd_step(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out);
 int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per_env,
                      int max_iter, int* iterations_out);
+/* vbd_step_batched followed by vbd_get_positions, in one blocking call (the
+ * reference drivers read every step's positions: run_mass_spring_parallel.py
+ * and run_cantilever.py:156).  When positions_out is page-locked, device-mapped
+ * host memory (cudaHostAlloc / cudaMallocHost, or torch pin_memory) and the
+ * solver runs in block mode, each environment's block writes its final
+ * positions there directly as it finishes, overlapping the transfer with the
+ * environments still running; otherwise the positions are copied after the
+ * step.  The values are the same either way. */
+int vbd_step_batched_to(vbd_solver* s, double dt, double tol, const double* tol_per_env,
+                        int max_iter, int* iterations_out, double* positions_out);
 
 /* Wait for the enqueued work; returns the status of the last step. */
 int vbd_sync(vbd_solver* s);

@@ -283,6 +283,34 @@ def test_incremental_potential_matches_oracle(precision, tol):
         assert abs(d_k - d_o) <= tol * abs(d_o), (e, d_k, d_o)
 
 
+@pytest.mark.parametrize("tiered,warm", [(False, False), (True, False), (True, True)])
+def test_step_into_host_array(tiered, warm):
+    """step(out=...) leaves the same positions as step() + positions():
+    written by the step kernels into a page-locked array, copied after the
+    step into a pageable one; sweep counts identical."""
+    import torch
+    from warpvbd_b200 import BatchedVBDSolver, warmstart
+    envs = scenes.env_batch(10, seed=6)
+    kw = dict(dx_tol=1e-7, max_iter=1000, cluster=4, tiered=tiered)
+    a, b = BatchedVBDSolver(envs, **kw), BatchedVBDSolver(envs, **kw)
+    if warm:
+        model = warmstart.load()
+        a.set_warmstart(model)
+        b.set_warmstart(model)
+    n = a.n_vertices
+    pinned = torch.empty((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    pageable = np.empty((n, 3))
+    for k in range(6):
+        ia = a.step(1e-3)
+        xa = a.positions()
+        out = pinned if k % 2 == 0 else pageable
+        out[:] = np.nan
+        ib = b.step(1e-3, out=out)
+        assert np.array_equal(ia, ib)
+        assert np.array_equal(xa, out), k
+    assert np.array_equal(a.velocities(), b.velocities())
+
+
 def test_downloads_into_caller_arrays():
     """positions(out=...) / DeviceArray.numpy(out=...) fill a caller array
     (e.g. page-locked) with exactly what a fresh download returns."""

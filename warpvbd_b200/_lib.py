@@ -91,6 +91,8 @@ SIGNATURES = {
     "vbd_step": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip]),
     "vbd_step_batched": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _d,
                                         ctypes.c_int, _ip]),
+    "vbd_step_batched_to": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _d,
+                                           ctypes.c_int, _ip, _d]),
     "vbd_sync": (ctypes.c_int, [_vp]),
     "vbd_get_iterations": (ctypes.c_int, [_vp, _ip]),
     "vbd_get_positions": (ctypes.c_int, [_vp, _d]),

@@ -127,13 +127,26 @@ class BatchedVBDSolver:
                 "sweeps": (rec[:, 3] >> np.uint64(8)).astype(np.int64),
                 "launch": (rec[:, 3] & np.uint64(0xFF)).astype(np.int64)}
 
-    def step(self, dt=1e-3, dx_tol=None, tol_per_env=None, max_iter=None, blocking=True):
+    def step(self, dt=1e-3, dx_tol=None, tol_per_env=None, max_iter=None, blocking=True,
+             out=None):
         """Step every environment; returns the per-environment sweep counts
-        (blocking) or None (enqueued only; see ``sync``)."""
+        (blocking) or None (enqueued only; see ``sync``).  ``out``: a
+        C-contiguous float64 [n_vertices, 3] array that receives the new
+        positions (blocking); page-locked memory (e.g. a torch tensor made
+        with pin_memory=True) is written by the step kernels themselves as
+        each environment finishes."""
         L = _lib.load()
         tol = self.dx_tol if dx_tol is None else dx_tol
         mi = self.max_iter if max_iter is None else max_iter
         tpe = None if tol_per_env is None else _lib.f64(tol_per_env, (self.n_env,))
+        if out is not None:
+            out = _host_out(out, self.n_vertices)
+            it = np.zeros(self.n_env, np.int32)
+            st = L.vbd_step_batched_to(self._h, float(dt), float(tol), _lib.ptr(tpe, "d"), int(mi),
+                                       it.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                       _lib.ptr(out, "d"))
+            self._after(st, it)
+            return it
         if blocking:
             it = np.zeros(self.n_env, np.int32)
             st = L.vbd_step_batched(self._h, float(dt), float(tol), _lib.ptr(tpe, "d"), int(mi),

@@ -478,6 +478,9 @@ struct vbd_solver {
   DevBuf<ushort4> d_rec_idx16;
   DevBuf<int4> d_tet_slot;
   DevBuf<int> d_tet_owner;
+  // vbd_step_batched_to: device-mapped pointer of the caller's page-locked
+  // output array during the enqueue of that step, else null
+  double* host_out = nullptr;
   // vbd_incremental_potential: candidate state (Real4) and per-env results
   DevBuf<unsigned char> d_xeval;
   DevBuf<double> d_pot;
@@ -570,6 +573,9 @@ struct vbd_solver {
     m.rec_tab = d_rec_tab.p;
     m.tet_slot = d_tet_slot.p;
     m.tet_owner = d_tet_owner.p;
+    m.host_out = host_out;
+    m.map = d_map.p;
+    m.rest = d_X.p;
     m.fmt = fmt;
     m.wstat = d_wstat.p;
     m.chunk_owner = d_chunk_owner.p;
@@ -1543,6 +1549,31 @@ int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per
   if (rc != VBD_OK) return rc;
   if (!iterations_out) return VBD_OK;
   return finish(s, iterations_out);
+}
+
+static int exchange(vbd_solver* s, const double* in, double* out, bool positions);
+
+int vbd_step_batched_to(vbd_solver* s, double dt, double tol, const double* tol_per_env,
+                        int max_iter, int* iterations_out, double* positions_out) {
+  if (!s || !iterations_out || !positions_out) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  NvtxRange nr("vbd_step");
+  DeviceGuard dg(s->device);
+  if (tol_per_env && s->mode != VBD_MODE_BLOCK)
+    return fail(VBD_ERR_UNSUPPORTED, "per-environment tolerances need block mode");
+  double* dptr = nullptr;
+  if (s->mode == VBD_MODE_BLOCK &&
+      cudaHostGetDevicePointer(reinterpret_cast<void**>(&dptr), positions_out, 0) != cudaSuccess) {
+    cudaGetLastError();  // not page-locked and mapped: copy after the step instead
+    dptr = nullptr;
+  }
+  s->host_out = dptr;
+  int rc = enqueue_step(s, dt, tol, tol_per_env, max_iter);
+  s->host_out = nullptr;
+  if (rc != VBD_OK) return rc;
+  rc = finish(s, iterations_out);
+  if (rc < 0 || dptr) return rc;
+  const int rc2 = exchange(s, nullptr, positions_out, true);
+  return rc2 != VBD_OK ? rc2 : rc;
 }
 
 int vbd_sync(vbd_solver* s) {

@@ -116,6 +116,13 @@ struct DevMesh {
   const float4* wstat;      // per vertex: h, log10(E / (rho h^2)), nu, valence / 20
   const int2* chunk_owner;  // per chunk: (colour index, environment)
   const float4* ws_pred;    // per vertex: predicted correction (xyz), w = 1 if predicted
+  // block mode, vbd_step_batched_to: the step's final positions in the
+  // caller's order (rest + displacement, float64 [n_vertices][3]) written
+  // by each environment's block(s) straight into page-locked host memory
+  // (device-mapped pointer), or null
+  double* host_out;
+  const int* map;      // caller vertex id -> renumbered id
+  const double* rest;  // rest positions, caller order, [n_vertices][3]
 };
 
 }  // namespace vbd

@@ -356,6 +356,19 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     reinterpret_cast<S4*>(m.u)[e.vbase + i] = un;
     end_vertex<SReal>(m, e.vbase + i, un, sc);
   }
+  if (m.host_out) {
+    // the environment's positions in the caller's order, one double per
+    // thread and consecutive threads on consecutive doubles (the caller's
+    // vertex ids of an environment are its renumbered range), written over
+    // the bus while other environments still run
+    double* out = m.host_out + 3 * (size_t)e.vbase;
+    const double* rest = m.rest + 3 * (size_t)e.vbase;
+    for (int k = rank * blockDim.x + threadIdx.x; k < 3 * e.nv; k += g * blockDim.x) {
+      const int j = k / 3, c = k - 3 * j;
+      const S4 un = local.load(m.map[e.vbase + j] - e.vbase);
+      out[k] = rest[k] + double(c == 0 ? un.x : (c == 1 ? un.y : un.z));
+    }
+  }
   if (stat) atomicOr(&s_stat, stat);
   __syncthreads();
   if (GROUP && g > 1) {
