@@ -57,3 +57,28 @@ def test_tip_csv_and_npz_roundtrip(tmp_path):
     assert sorted(d.keys()) == ["0", "1"] and np.allclose(d["1"], per_env[1])
     s = scenes.cantilever(20)
     assert np.allclose(io.tip_positions(s.vertices, s.tip), s.vertices[s.tip].mean(0))
+
+
+def test_state_checkpoint_roundtrip(tmp_path):
+    rng = np.random.default_rng(0)
+    x, v = rng.normal(size=(17, 3)), rng.normal(size=(17, 3))
+    p = tmp_path / "state.npz"
+    io.save_state(p, x, v, step=np.int64(12))
+    x2, v2, extra = io.load_state(p)
+    assert np.array_equal(x, x2) and np.array_equal(v, v2) and int(extra["step"]) == 12
+
+
+def test_step_log_jsonl(tmp_path):
+    from warpvbd_b200 import metrics
+    p = str(tmp_path / "run.jsonl")
+    log = metrics.StepLog(p, n_solved=[100, 50], dt=1e-3)
+    log.record([10, 20], 0.002)
+    log.record([5, 6], 0.001, note="x")
+    log.close()
+    rows = metrics.read(p)
+    assert [r["step"] for r in rows] == [1, 2]
+    assert rows[0]["sweeps_max"] == 20 and rows[0]["sweeps_mean"] == 15
+    assert abs(rows[0]["sim_s_per_wall_s"] - 1.0) < 1e-12       # 2 envs x 1 ms / 2 ms
+    assert abs(rows[0]["vertex_updates_per_s"] - (100 * 10 + 50 * 20) / 0.002) < 1e-6
+    assert abs(rows[1]["run_sim_s_per_wall_s"] - 2 * 2e-3 / 0.003) < 1e-12
+    assert rows[1]["note"] == "x"

@@ -1,4 +1,5 @@
-"""Output formats of the reference's drivers, for headless inspection.
+"""Output formats of the reference's drivers, for headless inspection, and
+state checkpoints.
 
 * Tip trajectories: ``save_tip_csv`` writes the per-step tip-face mean
   positions as CSV, one ``x,y,z`` row per step (examples/run_cantilever.py:177
@@ -74,4 +75,22 @@ def save_tip_npz(path, tip_positions_per_env):
     np.savez_compressed(path, **{str(k): np.asarray(v, np.float64) for k, v in items})
 
 
-__all__ = ["tet_surface", "write_obj", "tip_positions", "save_tip_csv", "save_tip_npz"]
+__all__ = ["tet_surface", "write_obj", "tip_positions", "save_tip_csv", "save_tip_npz",
+           "save_state", "load_state"]
+
+
+def save_state(path, positions, velocities, **extra):
+    """Checkpoint of a solver's state (x, v) -- all a VBD step depends on --
+    as a compressed npz (float64 [n, 3] each; `extra` arrays are stored too,
+    e.g. the step count).  Restore with load_state and the solver's
+    set_state(positions=..., velocities=...)."""
+    np.savez_compressed(path, positions=np.asarray(positions, np.float64),
+                        velocities=np.asarray(velocities, np.float64),
+                        **{k: np.asarray(v) for k, v in extra.items()})
+
+
+def load_state(path):
+    """(positions, velocities, extra dict) saved by save_state."""
+    with np.load(path) as z:
+        extra = {k: z[k] for k in z.files if k not in ("positions", "velocities")}
+        return z["positions"], z["velocities"], extra
