@@ -243,8 +243,9 @@ def cpu_sample(envs, batched):
 
 
 def run_reference(args, envs, desc, batched):
-    world, rank, _ = dist_init()
-    if rank != 0:
+    # a host-only run: no process group; under torchrun rank 0 alone times it
+    # and the other ranks exit at once
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     sample = cpu_sample(envs, batched)
     v, k, n, el = oracle_rate(sample, args.reference_budget_s, args.steps, warmup=args.warmup)
