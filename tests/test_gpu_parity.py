@@ -82,16 +82,19 @@ def test_fp64_graph_mode():
     assert np.array_equal(ig, io)
 
 
-def test_stvk_cantilever():
+@pytest.mark.parametrize("mode", ["block", "persist", "graph"])
+def test_stvk_cantilever(mode):
     s = scenes.cantilever(20)
-    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, material="stvk", mode="block")
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, material="stvk", mode=mode)
     assert worst < POS_TOL, worst
     assert orc.guard_hits == 0
+    assert np.abs(ig - io).max() <= 2
 
 
-def test_reference_default_damping():
+@pytest.mark.parametrize("mode", ["block", "persist", "graph"])
+def test_reference_default_damping(mode):
     s = scenes.cantilever(20)
-    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, kd=1.0, mode="block")
+    gpu, orc, xg, xo, ig, io, worst = run_pair(s, 100, kd=1.0, mode=mode)
     assert worst < POS_TOL, worst
 
 
