@@ -131,6 +131,24 @@ def test_batched_uneven_envs_match_per_env_oracle():
     assert len(set(its.tolist())) >= 1
 
 
+def test_batched_fp64_matches_oracle_tightly():
+    """The FP64 build of the batched (tiered) solver against the FP64 oracle,
+    environment by environment: within 1e-9 of the diagonal, same sweeps."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(6, seed=13)
+    b = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, precision="fp64", cluster=4,
+                         tiered=True)
+    orcs = [oracle.OracleSolver(**e.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7,
+                                max_iter=1000, guarded=True) for e in envs]
+    for k in range(15):
+        its = b.step(1e-3)
+        x = b.positions()
+        for e, (env, o) in enumerate(zip(envs, orcs)):
+            xo = o.step(None, 1e-3)
+            assert np.abs(x[b.env_slice(e)] - xo).max() / _diag(env.vertices) < 1e-9, (k, e)
+            assert int(its[e]) == o.last_iterations, (k, e)
+
+
 @pytest.mark.parametrize("cluster", [2, 4, 8])
 def test_single_env_split_over_a_cluster(cluster):
     """Block mode with the mesh replicated in every block of a cluster: each
