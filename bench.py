@@ -496,6 +496,23 @@ def run_ours(args, envs, desc, batched):
             es.close()
         line["plain_one_env_at_a_time"] = {
             "value": n_seq * DT / t_seq, "sample": "16 environments x 5 steps each"}
+        # the same batch over a longer stretch of its trajectory (the workload
+        # runs 1000 steps; sweep counts grow for the first few hundred): plain
+        # and warm-started, every step device-timed from the rest state
+        from warpvbd_b200 import warmstart
+        long = {}
+        for name, model in (("plain", None), ("warm_start", warmstart.load())):
+            ls = make_solver(envs, batched, local, warm=model,
+                             tuned=tuned_config(envs, batched, local, args.mode, not args.no_tune,
+                                                model is not None))
+            lms, lit, _ = timed_steps(ls, batched, args.long_steps, 0, local, flush)
+            long[name] = {"ms_per_step": float(lms.mean()),
+                          "iters_per_step": {"mean": float(lit.mean()), "max": int(lit.max())},
+                          "value": n_env * DT / (float(lms.mean()) * 1e-3)}
+            ls.close()
+        long["warm_start_speedup"] = (long["plain"]["ms_per_step"]
+                                      / long["warm_start"]["ms_per_step"])
+        line[f"batch_first_{args.long_steps}_steps"] = long
     if rank == 0 and world == 1 and batched and not args.no_secondary:
         # the plain single-mesh solver on the 160x16x16 cantilever
         cant = scenes.cantilever(160)
@@ -545,6 +562,8 @@ def main():
                     choices=["auto", "block", "graph", "hostloop", "persist"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--secondary-steps", type=int, default=30)
+    ap.add_argument("--long-steps", type=int, default=500,
+                    help="steps of the long plain / warm-started batch comparison")
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

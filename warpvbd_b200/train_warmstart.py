@@ -2,10 +2,11 @@
 
     python -m warpvbd_b200.train_warmstart [--out PATH] [--seed S] [--epochs E] [--lr LR]
 
-Generates ~2M samples from seeded plain-VBD rollouts (cantilever and
-mass-spring environments, E log-uniform in [1e5, 1e7] Pa, nu in [0.30, 0.48],
-random gravity direction per batch, N(0, 0.1^2) m/s initial velocity noise),
-trains the MLP with the project's CUDA kernels and writes the model
+Generates 4.6M samples from seeded plain-VBD rollouts of 1000 steps, every
+25th step recorded (cantilever and mass-spring environments, E log-uniform
+in [1e5, 1e7] Pa, nu in [0.30, 0.48], random gravity direction per batch,
+N(0, 0.1^2) m/s initial velocity noise), trains the MLP for 24 epochs with the
+project's CUDA kernels and writes the model
 (parameters and normalisation) (default: warpvbd_b200/data/warmstart_mlp.npz).  Prints a JSON
 summary with the dataset size, the training loss curve, R^2 and timings.
 """
@@ -20,11 +21,11 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=ws.DEFAULT_WEIGHTS)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--epochs", type=int, default=24)
     ap.add_argument("--batches", type=int, default=6)
     ap.add_argument("--envs", type=int, default=24)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--every", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000, help="steps per rollout")
+    ap.add_argument("--every", type=int, default=25, help="record every n-th step")
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--batch", type=int, default=4096, help="minibatch size")
     ap.add_argument("--fine", action="store_true",
