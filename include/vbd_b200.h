@@ -79,7 +79,7 @@ typedef struct vbd_solver vbd_solver;
  * at the same time (block_threads threads, shared memory for the largest of
  * them, so several blocks share an SM) */
 #define VBD_TIERED 0x4000
-/* block mode: thread blocks per cluster (1, 2, 4, 8, 16; 0 = automatic).  An
+/* block mode: thread blocks per cluster (1 to 16; 0 = automatic).  An
  * environment much heavier than the others is split over all blocks of one
  * cluster, which share its state through distributed shared memory. */
 #define VBD_CLUSTER_SHIFT 16

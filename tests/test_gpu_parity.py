@@ -149,7 +149,7 @@ def test_batched_fp64_matches_oracle_tightly():
             assert int(its[e]) == o.last_iterations, (k, e)
 
 
-@pytest.mark.parametrize("cluster", [2, 4, 8])
+@pytest.mark.parametrize("cluster", [2, 3, 4, 5, 6, 8])
 def test_single_env_split_over_a_cluster(cluster):
     """Block mode with the mesh replicated in every block of a cluster: each
     block updates its share of a colour and broadcasts it through distributed
@@ -160,6 +160,13 @@ def test_single_env_split_over_a_cluster(cluster):
     assert inf["cluster"] == cluster and inf["n_blocks"] == cluster
     assert worst < POS_TOL, worst
     assert np.abs(ig - io).max() <= 2, (ig, io)
+
+
+def test_cluster_size_above_16_is_refused():
+    from warpvbd_b200 import BatchedVBDSolver
+    from warpvbd_b200._lib import VBDError
+    with pytest.raises(VBDError, match="cluster size"):
+        BatchedVBDSolver(scenes.env_batch(2, seed=1), cluster=17)
 
 
 def test_batched_heavy_environment_split():
@@ -224,7 +231,7 @@ def test_nonconvergence_warning_and_nonfinite(capsys):
         sol.step(bad, 1e-3)
 
 
-@pytest.mark.parametrize("cluster,threads", [(4, 256), (8, 128), (2, 512)])
+@pytest.mark.parametrize("cluster,threads", [(4, 256), (8, 128), (2, 512), (5, 512), (6, 256)])
 def test_tiered_launch_is_bit_identical_to_one_launch(cluster, threads):
     """Heavy environments on clusters in one launch, the rest one block each
     in a concurrent second launch: every environment's arithmetic is the

@@ -694,6 +694,7 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
 //   one block              sweeps * (slots + 8300)
 //   split over C blocks    sweeps * (slots / C + I_C),
 //                          I_C = 10300 / 11200 / 12200 / 16500 for C = 2 / 4 / 8 / 16
+//                          (interpolated for the other sizes)
 // (the fixed part is the per-colour barrier and dependency chain: a
 // 7K-slot environment costs 29 us per sweep, a 44K-slot one 110 us; a
 // 68K-slot environment 129 / 77 / 49 / 36 / 36 us on 1 / 2 / 4 / 8 / 16
@@ -707,12 +708,23 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
 // and an environment whose count jumps while it runs alone on one block sets
 // the step time.  Blocks are listed longest first, which the block scheduler
 // then starts first.
+// I_C of the duration model: measured at C = 2, 4, 8, 16, linear in C between
+// those points (C = 3, 5-7, 9-15).
+double split_overhead(int C) {
+  static const double c[4] = {2.0, 4.0, 8.0, 16.0};
+  static const double v[4] = {10300.0, 11200.0, 12200.0, 16500.0};
+  if (C <= 2) return v[0];
+  for (int i = 1; i < 4; ++i)
+    if (C <= c[i]) return v[i - 1] + (v[i] - v[i - 1]) * (C - c[i - 1]) / (c[i] - c[i - 1]);
+  return v[3];
+}
+
 void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
                std::vector<int4>& work2) {
   const int n = s->n_env, C = s->cluster;
   work2.clear();
   const double a1 = 8300.0;
-  const double aC = C == 2 ? 10300.0 : (C == 4 ? 11200.0 : (C == 8 ? 12200.0 : 16500.0));
+  const double aC = split_overhead(C);
   std::vector<double> d1(n), dC(n), m1(n), mC(n);  // high and mean estimates
   const bool hist = s->env_sweeps.size() == (size_t)n && s->env_sweeps_mean.size() == (size_t)n &&
                     s->env_sweeps_decay.size() == (size_t)n;
@@ -891,9 +903,9 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   s->mode = mode;
   const bool block_mode = mode == VBD_MODE_BLOCK;
   const int cl = (flags >> VBD_CLUSTER_SHIFT) & 0x1F;
-  if (cl != 0 && cl != 1 && cl != 2 && cl != 4 && cl != 8 && cl != 16) {
+  if (cl > 16) {
     delete s;
-    return fail(VBD_ERR_INVALID_ARG, "cluster size must be 1, 2, 4, 8 or 16");
+    return fail(VBD_ERR_INVALID_ARG, "cluster size must be 0 (automatic) or 1 to 16");
   }
   s->cluster = !block_mode ? 1 : (cl ? cl : (s->n_env > 1 ? 4 : (V > 512 ? 8 : 1)));
   s->replan = block_mode && s->n_env > 1 && s->cluster > 1;

@@ -159,7 +159,7 @@ class VBDSolver:
       mode       "auto", "block", "graph", "hostloop" or "persist" (see include/vbd_b200.h)
       tpv, block_threads   launch shape (0 = automatic)
       cluster    block mode: spread the mesh over this many thread blocks of one
-                 cluster (1, 2, 4, 8, 16; 0 = automatic)
+                 cluster (1 to 16; 0 = automatic)
       order_index  keep ascending vertex index inside a colour (default: by valence)
       tune       pick mode / tpv / block_threads / cluster / order_index with the
                  autotuner (warpvbd_b200.autotune; measured once per mesh and GPU
