@@ -4,8 +4,10 @@ Default workload (``--workload batch256``): 256 mass-spring environments of
 uneven size drawn from seed 0 (cube edge 7-15 voxels, column 5-30 voxels,
 1 cm voxels, E log-uniform 1e5-1e6 Pa, nu 0.35-0.48, rho 1000, the column's
 top face fixed, gravity -z), Stable Neo-Hookean, dt = 1 ms, tol 1e-7, at most
-1000 sweeps per step; fp32 arithmetic with fp64 positions.  All environments
-advance in one launch per step, each with its own convergence test.
+1000 sweeps per step, 1000 steps; arithmetic and state in fp64 (the
+reference's precision; ``--precision mixed`` for fp32 per-slot arithmetic).
+All environments advance in one launch per step, each with its own
+convergence test.
 
 A "step" is one implicit-Euler time step of every environment (inertia guess,
 colour sweeps until max|dx_x+dx_y+dx_z| < tol, velocity update).
@@ -15,6 +17,14 @@ the data path).  Other workloads: cantilever20/40/80/160/320, massspring.
 The headline batched run starts every step from the learned warm start (the
 metric's "warm-start + batched" form); plain batched VBD is timed beside it
 (``plain_batched``, with the ratio; ``--warmstart off`` swaps the two).
+
+The cost of a step changes along the 1000-step trajectory (the sweep counts
+grow over the first few hundred steps as the environments swing), so the
+timed window does not start from rest: every timed run first advances its
+solver ``--start-step`` steps (default 500, the middle of the trajectory)
+untimed, then takes the warm-up and timed steps.  ``batch_1000_steps``
+reports the whole trajectory from rest, plain and warm-started, every step
+device-timed.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
   python bench.py --impl reference ...   # FP64 CPU oracle on the host cores
@@ -44,25 +54,49 @@ MAX_ITER = 1000
 MODE_NAMES = {0x100: "block", 0x200: "graph", 0x300: "hostloop", 0x400: "persist"}
 
 
-def make_workload(name):
+PRECISION_TEXT = {"fp64": "fp64 arithmetic and state",
+                  "mixed": "fp32 per-slot arithmetic, fp64 state", "fp32": "fp32"}
+DTYPES = {"fp64": "f64", "mixed": "f32", "fp32": "f32"}
+
+
+def make_workload(name, precision="fp64"):
     """-> (list of Scene environments, description, batched?)"""
+    p = PRECISION_TEXT[precision]
     if name == "batch256":
         return (scenes.env_batch(256, seed=0),
-                "256 uneven mass-spring envs (seed 0), SNH, fp32 math / fp64 state", True)
+                f"256 uneven mass-spring envs (seed 0), SNH, {p}", True)
     if name.startswith("cantilever"):
         n = int(name[len("cantilever"):])
-        return [scenes.cantilever(n)], f"cantilever {n}x{n // 10}x{n // 10} SNH, fp32 math / fp64 state", False
+        return [scenes.cantilever(n)], f"cantilever {n}x{n // 10}x{n // 10} SNH, {p}", False
     if name == "massspring":
-        return [scenes.mass_spring(11, 20)], "mass-spring 11^3 cube + 1x1x20 column SNH", False
+        return [scenes.mass_spring(11, 20)], f"mass-spring 11^3 cube + 1x1x20 column SNH, {p}", \
+            False
     raise SystemExit(f"unknown workload {name}")
 
 
 def sweep_bytes(s):
     """Algorithmic bytes of one sweep of one mesh: sum over solved vertices of
-    44 + 104 k_v (44 B of per-vertex state, 104 B per incident tet)."""
+    B(v) = 44 + 104 k_v (fp32 storage, no reuse between vertices credited:
+    44 B of per-vertex state -- x read and written, inertia target, lumped
+    mass, adjacency offset -- and per incident tet 104 B: tet id, 4 vertex
+    ids, Dm^-1, rest volume, (mu', lambda'), three neighbour positions)."""
     k = np.bincount(s.tets.reshape(-1), minlength=s.n_vertices)
     solved = s.active & (k > 0)
     return float((44 + 104 * k[solved]).sum()), int(solved.sum()), int(k[solved].sum())
+
+
+def warm_stage_bytes(s):
+    """Algorithmic bytes of the learned warm start's energy check of one mesh
+    (the inertia guess and the full prediction compared in one pass over the
+    mesh's tet list, fp32 storage like sweep_bytes): per tet with a solved
+    vertex 176 B (4 vertex ids 16, Dm^-1 36, volume 4, (mu', lambda') 8, the
+    four positions 48 and predictions 64), per solved vertex 44 B (position,
+    inertia target, lumped mass, prediction).  The line search's further
+    candidates (taken when the first raises the energy) are not counted."""
+    k = np.bincount(s.tets.reshape(-1), minlength=s.n_vertices)
+    solved = s.active & (k > 0)
+    tets_solved = int(solved[s.tets].any(axis=1).sum())
+    return float(176 * tets_solved + 44 * int(solved.sum()))
 
 
 _REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
@@ -265,7 +299,7 @@ def run_reference(args, envs, desc, batched):
     print(json.dumps(line), flush=True)
 
 
-def tuned_config(envs, batched, local, mode="auto", use=True, warm=False):
+def tuned_config(envs, batched, local, mode="auto", use=True, warm=False, precision="fp64"):
     """The autotuner's cached launch shape for this workload on this GPU
     (warpvbd_b200/data/autotune_b200.json or the user cache), or None.
     `warm`: the shape tuned with the learned warm start on (falls back to
@@ -275,25 +309,35 @@ def tuned_config(envs, batched, local, mode="auto", use=True, warm=False):
     from warpvbd_b200 import autotune
     dev = f"cuda:{local}"
     if batched:
-        return ((autotune.cached_batched(envs, device=dev, warm=True) if warm else None)
-                or autotune.cached_batched(envs, device=dev))
-    return autotune.cached_single(envs[0].solver_kwargs(), device=dev)
+        return ((autotune.cached_batched(envs, device=dev, warm=True, precision=precision)
+                 if warm else None)
+                or autotune.cached_batched(envs, device=dev, precision=precision))
+    return autotune.cached_single(envs[0].solver_kwargs(), device=dev, precision=precision)
 
 
-def make_solver(envs, batched, local, mode="auto", warm=None, tuned=None):
+def make_solver(envs, batched, local, mode="auto", warm=None, tuned=None, precision="fp64"):
     if batched:
         from warpvbd_b200 import BatchedVBDSolver
         sol = BatchedVBDSolver(envs, dx_tol=TOL, max_iter=MAX_ITER, device=f"cuda:{local}",
-                               **(tuned or {}))
+                               precision=precision, **(tuned or {}))
     else:
         from warpvbd_b200 import VBDSolver
         s = envs[0]
         shape = tuned or {"mode": mode}
         sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL,
-                        max_iter=MAX_ITER, device=f"cuda:{local}", **shape)
+                        max_iter=MAX_ITER, device=f"cuda:{local}", precision=precision, **shape)
     if warm is not None:
         sol.set_warmstart(warm)
     return sol
+
+
+def solver_for(args, envs, batched, local, warm, precision=None):
+    """A solver of the workload with its tuned launch shape (and the tuned
+    shape's description)."""
+    precision = precision or args.precision
+    tuned = tuned_config(envs, batched, local, args.mode, not args.no_tune, warm is not None,
+                         precision)
+    return make_solver(envs, batched, local, args.mode, warm, tuned, precision), tuned
 
 
 def warm_params(args, batched):
@@ -312,15 +356,20 @@ def step_async(sol, batched):
         sol.step(sol.old_positions, DT, blocking=False)
 
 
+def advance(sol, batched, steps):
+    """Untimed steps (the lead-in to the timed window)."""
+    for _ in range(steps):
+        step_async(sol, batched)
+        sol.sync()
+
+
 def timed_steps(sol, batched, steps, warmup, local, flush, sample_clocks=False, detail=None):
     """Per-step CUDA-event times (ms) and per-step sweep counts.  `detail`
     (a dict) receives the step kernels' own CUDA-event times (the library
     records events around them on its stream) and the kernels launched."""
     import torch
     stream = torch.cuda.ExternalStream(sol.stream, device=local)
-    for _ in range(warmup):
-        step_async(sol, batched)
-        sol.sync()
+    advance(sol, batched, warmup)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(steps)]
     iters = []
@@ -343,25 +392,30 @@ def timed_steps(sol, batched, steps, warmup, local, flush, sample_clocks=False, 
     return ms, np.stack(iters), clocks
 
 
+def max_over_ranks(x, world, local):
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], device=f"cuda:{local}")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, envs, desc, batched):
     import torch
     world, rank, local = dist_init()
     torch.cuda.set_device(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     warm = warm_params(args, batched)
-    tuned = tuned_config(envs, batched, local, args.mode, not args.no_tune, warm is not None)
-    sol = make_solver(envs, batched, local, args.mode, warm, tuned)
+    sol, tuned = solver_for(args, envs, batched, local, warm)
     info = sol.info()
+    advance(sol, batched, args.start_step)
     if world > 1:
         torch.distributed.barrier()
     detail = {}
     ms, iters, clocks = timed_steps(sol, batched, args.steps, args.warmup, local, flush,
                                     sample_clocks=True, detail=detail)
-    total_ms = float(ms.sum())
-    if world > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(ms.sum()), world, local)
     n_env = len(envs)
     value = world * n_env * args.steps * DT / (total_ms * 1e-3)
 
@@ -390,34 +444,35 @@ def run_ours(args, envs, desc, batched):
     e2e = world * n_env * args.e2e_steps * DT / e2e_s
 
     # roofline of the dominant kernel: algorithmic bytes of the sweeps it ran
+    # (and of the warm start's energy check) over its own CUDA-event time
     per_env = [sweep_bytes(e) for e in envs]
     b_sweep = np.array([p[0] for p in per_env])
     slots = np.array([p[2] for p in per_env])
     solved = np.array([p[1] for p in per_env])
+    b_warm = np.array([warm_stage_bytes(e) for e in envs]) if warm is not None else 0.0
     mode = MODE_NAMES[info["mode"]]
-    # sweeps, plus the energy pass over every slot (both potentials in one
-    # pass) when the warm start compares the prediction with the inertia
-    # guess; the rare extra passes of the line search are not counted
-    passes = iters + (1 if warm is not None else 0)
-    alg_bytes = float((passes * b_sweep[None, :]).sum())
+    alg_bytes = float((iters * b_sweep[None, :]).sum()) + args.steps * float(np.sum(b_warm))
     # the dominant kernel's own time: the library's events around the step
     # kernels (both tiers; without the warm-start feature / inference kernels)
     kernel_ms = float(np.sum(detail["kernel_ms"]))
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     kernel = {"block": "env_step_kernel", "persist": "persist_kernel"}.get(mode, "color_kernel")
-    # the capture of the same setting (warm-started or plain), else the other
-    tps = (profile_traffic_per_slot(kernel, args.workload + ".warm") if warm is not None
-           else None) or profile_traffic_per_slot(kernel, args.workload)
-    traffic = None if tps is None else tps * float((passes * slots[None, :]).sum()) / args.steps
+    prof = f"{args.workload}.{args.precision}" + (".warm" if warm is not None else "")
+    tps = profile_traffic_per_slot(kernel, prof)
+    traffic = None if tps is None else tps * float((iters * slots[None, :]).sum()) / args.steps
     launches = int(np.sum(detail["launches"]))  # counted by the library, per step
     line = {"metric": "sim-s/wall-s", "value": value, "unit": "sim-s/wall-s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": DTYPES[args.precision], "data": "synthetic",
             "config": {"workload": desc, "n_env": n_env, "vertices": n_vertices,
                        "tets": int(sum(e.n_tets for e in envs)), "dt": DT, "tol": TOL,
-                       "max_iter": MAX_ITER, "mode": mode, "tpv": info["tpv"],
+                       "max_iter": MAX_ITER, "precision": args.precision,
+                       "timed_window": f"steps {args.start_step + args.warmup + 1}-"
+                                       f"{args.start_step + args.warmup + args.steps} "
+                                       "of the trajectory from rest",
+                       "mode": mode, "tpv": info["tpv"],
                        "block_threads": info["block_threads"],
                        "parallelism": f"replicas x{world}",
                        "warm_start": warm is not None, "cluster": info["cluster"],
@@ -434,6 +489,14 @@ def run_ours(args, envs, desc, batched):
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes / args.steps,
+                         "bytes_model": "B(v) = 44 + 104 k_v per vertex update, fp32 storage; "
+                                        "warm-start check: 176 B per tet + 44 B per vertex",
+                         "limiter": "issue and latency: the records and slots stay in L2 and "
+                                    "the positions in shared memory, DRAM traffic is a small "
+                                    "fraction of the algorithmic bytes (ncu summary in "
+                                    "profiles/)" if mode == "block" else
+                                    "latency: the per-colour dependency chain and grid "
+                                    "barriers (ncu summary in profiles/)",
                          "kernel_ms_per_step": kernel_ms / args.steps},
             "e2e": {"value": e2e, "unit": "sim-s/wall-s",
                     "h2d_bytes_per_step": 24 * n_vertices,
@@ -446,7 +509,7 @@ def run_ours(args, envs, desc, batched):
         v, k, n, el = oracle_rate(sample, args.cpu_budget_s, 50)
         line["cpu_baseline"] = {
             "value": v, "unit": "sim-s/wall-s", "cores": n, "kind": "port",
-            "sample": f"{k} whole steps of {len(sample)} environment(s) "
+            "sample": f"{k} whole steps from rest of {len(sample)} environment(s) "
                       + ("concatenated into one mesh " if batched else "")
                       + f"({el:.1f} s), FP64 C oracle, OpenMP {n} threads"}
         # the reference's Warp CPU device runs its kernels on one thread: the
@@ -454,23 +517,20 @@ def run_ours(args, envs, desc, batched):
         v1, k1, _, el1 = oracle_rate(sample[:1], min(5.0, args.cpu_budget_s), 50, threads=1)
         line["cpu_baseline"]["single_thread"] = {
             "value": v1, "sample": f"{k1} whole steps of 1 environment ({el1:.1f} s), 1 thread"}
+    sol.close()
     if batched and not args.no_secondary:
-        # the same batch with the learned warm start toggled (same timing
-        # method); every rank takes this path, so the collectives match
+        # the same batch with the learned warm start toggled (same window,
+        # same timing method); every rank takes this path, so the collectives
+        # match
         from warpvbd_b200 import warmstart
-        sol.close()
         other = None if warm is not None else warmstart.load()
-        ps = make_solver(envs, batched, local, warm=other,
-                         tuned=tuned_config(envs, batched, local, args.mode, not args.no_tune,
-                                            other is not None))
+        ps, _ = solver_for(args, envs, batched, local, other)
+        advance(ps, batched, args.start_step)
         pms, pit, _ = timed_steps(ps, batched, args.steps, args.warmup, local, flush)
-        pt = float(pms.sum())
-        if world > 1:
-            t = torch.tensor([pt], device=f"cuda:{local}")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            pt = float(t.item())
-        ppass = pit + (1 if other is not None else 0)
-        pbytes = float((ppass * b_sweep[None, :]).sum())
+        pt = max_over_ranks(float(pms.sum()), world, local)
+        pbytes = float((pit * b_sweep[None, :]).sum())
+        if other is not None:
+            pbytes += args.steps * float(np.sum([warm_stage_bytes(e) for e in envs]))
         pv = world * n_env * args.steps * DT / (pt * 1e-3)
         key = "warm_start_batched" if other is not None else "plain_batched"
         pinfo = ps.info()
@@ -489,51 +549,61 @@ def run_ours(args, envs, desc, batched):
         # sample of the batch: what the batch costs without batching
         t_seq, n_seq = 0.0, 0
         for env in envs[:16]:
-            es = make_solver([env], False, local)
+            es = make_solver([env], False, local, precision=args.precision)
             ems, _, _ = timed_steps(es, False, 5, 3, local, flush)
             t_seq += float(ems.sum()) * 1e-3
             n_seq += 5
             es.close()
         line["plain_one_env_at_a_time"] = {
-            "value": n_seq * DT / t_seq, "sample": "16 environments x 5 steps each"}
-        # the same batch over a longer stretch of its trajectory (the workload
-        # runs 1000 steps; sweep counts grow for the first few hundred): plain
-        # and warm-started, every step device-timed from the rest state
+            "value": n_seq * DT / t_seq, "sample": "16 environments x 5 steps each, from rest"}
+        # the workload's whole trajectory from rest, plain and warm-started,
+        # every step device-timed
         from warpvbd_b200 import warmstart
         long = {}
         for name, model in (("plain", None), ("warm_start", warmstart.load())):
-            ls = make_solver(envs, batched, local, warm=model,
-                             tuned=tuned_config(envs, batched, local, args.mode, not args.no_tune,
-                                                model is not None))
+            ls, _ = solver_for(args, envs, batched, local, model)
             lms, lit, _ = timed_steps(ls, batched, args.long_steps, 0, local, flush)
             long[name] = {"ms_per_step": float(lms.mean()),
                           "iters_per_step": {"mean": float(lit.mean()), "max": int(lit.max())},
-                          "value": n_env * DT / (float(lms.mean()) * 1e-3)}
+                          "value": n_env * DT / (float(lms.mean()) * 1e-3),
+                          "ms_per_step_by_100_steps": [
+                              round(float(lms[i:i + 100].mean()), 4)
+                              for i in range(0, args.long_steps, 100)]}
             ls.close()
         long["warm_start_speedup"] = (long["plain"]["ms_per_step"]
                                       / long["warm_start"]["ms_per_step"])
-        line[f"batch_first_{args.long_steps}_steps"] = long
+        line[f"batch_{args.long_steps}_steps"] = long
+        if args.precision != "mixed":
+            # the fp32-arithmetic mode on the same window, for comparison:
+            # faster, but its trajectories drift from the fp64 ones
+            ms_, _ = solver_for(args, envs, batched, local, warm, precision="mixed")
+            advance(ms_, batched, args.start_step)
+            mms, mit, _ = timed_steps(ms_, batched, args.steps, args.warmup, local, flush)
+            line["mixed_precision_same_window"] = {
+                "value": n_env * args.steps * DT / (float(mms.sum()) * 1e-3),
+                "ms_per_step": float(mms.mean()), "iters_per_step": float(mit.mean()),
+                "warm_start": warm is not None}
+            ms_.close()
     if rank == 0 and world == 1 and batched and not args.no_secondary:
-        # the plain single-mesh solver on the 160x16x16 cantilever
+        # the plain single-mesh solver on the 160x16x16 cantilever (from rest)
         cant = scenes.cantilever(160)
-        cs = make_solver([cant], False, local,
-                         tuned=tuned_config([cant], False, local, "auto", not args.no_tune))
+        cs, _ = solver_for(args, [cant], False, local, None)
         cdet = {}
         cms, cit, _ = timed_steps(cs, False, args.secondary_steps, 3, local, flush, detail=cdet)
         cb, csolved, _ = sweep_bytes(cant)
         t = float(cms.sum()) * 1e-3
+        tk = float(np.sum(cdet["kernel_ms"])) * 1e-3
         line["cantilever160"] = {
             "sim_s_per_wall_s": args.secondary_steps * DT / t,
             "ms_per_step": 1e3 * t / args.secondary_steps,
             "iters_per_step": float(cit.mean()), "mode": MODE_NAMES[cs.info()["mode"]],
             "vertex_updates_per_s": csolved * float(cit.sum()) / t,
-            "roofline_frac": cb * float(cit.sum()) / t / 1e9 / peak,
-            "kernel_ms_per_step": float(np.mean(cdet["kernel_ms"]))}
+            "roofline_frac": cb * float(cit.sum()) / tk / 1e9 / peak,
+            "kernel_ms_per_step": 1e3 * tk / args.secondary_steps}
         cs.close()
         # the same cantilever with the learned warm start (persistent mode)
         from warpvbd_b200 import warmstart
-        ws_ = make_solver([cant], False, local, warm=warmstart.load(),
-                          tuned=tuned_config([cant], False, local, "auto", not args.no_tune))
+        ws_, _ = solver_for(args, [cant], False, local, warmstart.load())
         wdet = {}
         wms, wit, _ = timed_steps(ws_, False, args.secondary_steps, 3, local, flush, detail=wdet)
         tw = float(wms.sum()) * 1e-3
@@ -562,8 +632,11 @@ def main():
                     choices=["auto", "block", "graph", "hostloop", "persist"])
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--secondary-steps", type=int, default=30)
-    ap.add_argument("--long-steps", type=int, default=500,
-                    help="steps of the long plain / warm-started batch comparison")
+    ap.add_argument("--long-steps", type=int, default=1000,
+                    help="steps of the whole-trajectory plain / warm-started batch comparison")
+    ap.add_argument("--start-step", type=int, default=500,
+                    help="untimed steps from rest before the warm-up and timed steps")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
     ap.add_argument("--cpu-budget-s", type=float, default=20.0)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -576,7 +649,7 @@ def main():
                          "timed beside it as plain_batched / warm_start_batched")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    envs, desc, batched = make_workload(args.workload)
+    envs, desc, batched = make_workload(args.workload, args.precision)
     if args.impl == "reference":
         run_reference(args, envs, desc, batched)
     else:

@@ -179,6 +179,11 @@ int vbd_step_batched_to(vbd_solver* s, double dt, double tol, const double* tol_
 int vbd_sync(vbd_solver* s);
 /* Sweep counts of the last step, n_env entries. */
 int vbd_get_iterations(vbd_solver* s, int* iterations_out);
+/* Per environment (n_env entries): the largest |dx| component of the last
+ * step's final sweep when that step used all max_iter sweeps, else NaN.
+ * Replaces the value the reference prints in its non-convergence warning,
+ * abs(dxs.numpy()).max() (src/vbd_solver.py:581-582). */
+int vbd_get_final_dx(vbd_solver* s, double* final_dx_out);
 
 /* State in the caller's vertex order, float64 [n_vertices][3].  A host
  * pointer to page-locked memory is copied directly (fastest).  Setting the
@@ -282,12 +287,15 @@ int vbd_mlp_adam(float* params, const float* grad, float* m, float* v, int n, fl
  * The sweep's scratch (step parameters, loop control, one convergence partial
  * per thread block) lives in one static device array of 131,200 bytes that
  * every GPU loading the library holds until exit: a mesh whose sweep needs
- * more than 16,384 thread blocks (a largest colour of about one million
- * vertices at 4 lanes per vertex) is rejected with VBD_ERR_UNSUPPORTED, as
- * is a batched solver.  All calls share the array: calls whose GPU work
- * overlaps (other streams, other host threads) race and must be serialised.
- * The first call on a device resolves the array's device address, so make it
- * before any stream capture on that device. */
+ * more than 16,384 thread blocks, summed over all its colours (each block
+ * takes 8 chunks of 32 / tpv vertices: about one million solved vertices in
+ * the whole mesh at 4 lanes per vertex), is rejected with
+ * VBD_ERR_UNSUPPORTED, as is a batched solver.  All calls share the array:
+ * calls whose GPU work overlaps (other streams, other host threads) race and
+ * must be serialised.  The first call on a device resolves the array's device
+ * address, so make it before any stream capture on that device.  The step is
+ * always a plain one: with the learned warm start enabled the prediction is
+ * not used.  vbd_get_info reports its kernel time and launch count. */
 int vbd_step_noalloc(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out);
 
 #ifdef __cplusplus

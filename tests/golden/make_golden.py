@@ -1,7 +1,7 @@
 """Generate the golden mesh / colouring fixtures from the reference's own code.
 
-This script is run by hand in a container that holds the reference checkout
-(mmichelis/WarpVBD) at /root/reference.  It imports, unchanged:
+This script is run by hand in a container that holds a checkout of the
+reference (mmichelis/WarpVBD).  It imports, unchanged:
 
   * src/_utils.py     voxel2hex (:35-89), hex2tets (:92-108)
   * src/coloring.py   compute_adjacency_dict (:24-38), graph_coloring (:40-72)
@@ -16,7 +16,8 @@ Outputs (committed):
                             for every mesh, including the large cantilevers
                             whose arrays are too big to commit.
 
-Run:  python tests/golden/make_golden.py [--large]
+Run:  python tests/golden/make_golden.py --ref <checkout> [--large]
+      (``--ref`` defaults to the environment variable WARPVBD_REFERENCE)
 """
 import argparse
 import hashlib
@@ -29,13 +30,12 @@ import contextlib
 
 import numpy as np
 
-REF_SRC = "/root/reference/src"
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def _import_reference():
+def _import_reference(ref_src):
     sys.modules.setdefault("warp", types.ModuleType("warp"))
-    sys.path.insert(0, REF_SRC)
+    sys.path.insert(0, ref_src)
     import _utils as ref_utils  # noqa: E402
     import coloring as ref_coloring  # noqa: E402
     return ref_utils, ref_coloring
@@ -70,8 +70,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--large", action="store_true",
                     help="also hash the 160x16x16 and 320x32x32 cantilevers")
+    ap.add_argument("--ref", default=os.environ.get("WARPVBD_REFERENCE"),
+                    help="checkout of mmichelis/WarpVBD (default: $WARPVBD_REFERENCE)")
     args = ap.parse_args()
-    ref_utils, ref_coloring = _import_reference()
+    if not args.ref:
+        ap.error("give --ref or set WARPVBD_REFERENCE")
+    ref_utils, ref_coloring = _import_reference(os.path.join(os.path.abspath(args.ref), "src"))
 
     arrays = {}
     hashes = {}

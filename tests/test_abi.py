@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from warpvbd_b200 import _lib
 
@@ -76,3 +77,13 @@ def test_native_coloring_rejects_more_than_256_colours():
         assert col.max() < 256
     with pytest.raises(Exception):
         color_tets(np.array([[0, 1, 2, -5]], np.int32))
+
+
+def test_cluster_flags_refuse_out_of_range_sizes():
+    """The cluster field is 5 bits wide: 0 (automatic) and 1..16 are shifted
+    in, anything else is refused before it can spill into other bits."""
+    assert _lib.cluster_flags(0) == 0
+    assert _lib.cluster_flags(16) == 16 << _lib.CLUSTER_SHIFT
+    for bad in (17, 32, 48, -1, 2.5):
+        with pytest.raises(ValueError, match="cluster must be"):
+            _lib.cluster_flags(bad)

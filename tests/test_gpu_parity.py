@@ -163,10 +163,28 @@ def test_single_env_split_over_a_cluster(cluster):
 
 
 def test_cluster_size_above_16_is_refused():
-    from warpvbd_b200 import BatchedVBDSolver
+    """The Python front ends refuse a cluster size outside 0..16 before
+    shifting it into the flags; the C ABI refuses 17..31 in the 5-bit field
+    and any flag bit above it (a size of 32 or more, or a negative one)."""
+    import ctypes
+    from warpvbd_b200 import BatchedVBDSolver, _lib
     from warpvbd_b200._lib import VBDError
-    with pytest.raises(VBDError, match="cluster size"):
-        BatchedVBDSolver(scenes.env_batch(2, seed=1), cluster=17)
+    envs = scenes.env_batch(2, seed=1)
+    for c in (17, 32, 48, -1):
+        with pytest.raises(ValueError, match="cluster must be"):
+            BatchedVBDSolver(envs, cluster=c)
+    s = envs[0]
+    L = _lib.load()
+    X, tets = _lib.f64(s.vertices), _lib.i32(s.tets)
+    rho, E, nu = _lib.f64(s.density), _lib.f64(s.youngs), _lib.f64(s.poisson)
+    base = _lib.MATERIAL_SNH | _lib.PRECISION_FP64 | _lib.MODE_BLOCK
+    for bits in (17 << _lib.CLUSTER_SHIFT, 32 << _lib.CLUSTER_SHIFT, 1 << 28):
+        h = ctypes.c_void_p()
+        st = L.vbd_create(_lib.ptr(X, "d"), X.shape[0], _lib.ptr(tets, "i"), tets.shape[0],
+                          _lib.ptr(rho, "d"), _lib.ptr(E, "d"), _lib.ptr(nu, "d"), None, 0.0,
+                          None, None, base | bits, 0, 0, 0, ctypes.byref(h))
+        assert st == _lib.ERR_INVALID_ARG, (bits, st)
+        assert b"cluster size" in L.vbd_last_error_message()
 
 
 def test_batched_heavy_environment_split():
@@ -360,6 +378,33 @@ def test_checkpoint_resume(tmp_path):
     for _ in range(5):
         assert np.array_equal(a.step(1e-3), b.step(1e-3))
     assert np.abs(a.positions() - b.positions()).max() < 1e-9
+
+
+def test_checkpoint_resume_warm_started_batch(tmp_path):
+    """The learned warm start also reads the previous step's inertia target,
+    which a checkpoint of (x, v) does not hold: a warm-started batch restored
+    into a fresh solver continues within the solver's tolerance of the
+    uninterrupted run, not bit for bit (io.save_state's docstring)."""
+    from warpvbd_b200 import BatchedVBDSolver, io, warmstart
+    envs = scenes.env_batch(6, seed=8)
+    model = warmstart.load()
+    a = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000)
+    a.set_warmstart(model)
+    for _ in range(5):
+        a.step(1e-3)
+    io.save_state(tmp_path / "ck.npz", a.positions(), a.velocities(), step=5)
+    b = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000)
+    b.set_warmstart(model)
+    x, v, _ = io.load_state(tmp_path / "ck.npz")
+    b.set_state(positions=x, velocities=v)
+    for _ in range(5):
+        a.step(1e-3)
+        b.step(1e-3)
+    xa, xb = a.positions(), b.positions()
+    worst = max(np.abs(xa[a.env_slice(e)] - xb[a.env_slice(e)]).max() / _diag(envs[e].vertices)
+                for e in range(len(envs)))
+    print(f"warm-started resume: largest difference {worst:.2e} of the diagonal")
+    assert worst < 1e-4
 
 
 def test_downloads_into_caller_arrays():

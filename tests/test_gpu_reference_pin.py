@@ -1,0 +1,237 @@
+"""The CUDA solver against trajectories of the reference's own code, and
+against the FP64 oracle over whole configured trajectories (GPU tests).
+
+Fixtures (tests/golden):
+  ref_trajectories.npz  made by make_ref_trajectories.py, which runs the
+                        reference's unchanged src/vbd_solver.py (through a
+                        pure-Python Warp stand-in): the 20x2x2 cantilever
+                        with SNH (300 steps), StVK (100), the reference's
+                        default damping k_d = 1 (40), max_iter = 3 (8), and a
+                        small mass-spring (60 steps);
+  oracle_long.npz       made by make_oracle_long.py with the FP64 oracle:
+                        mass-spring 11^3 + 1x1x20 for 1000 steps, the
+                        160x16x16 cantilever (SNH 300 steps, StVK 100), and
+                        32 of the 256 batch environments for 300 steps.
+
+Bars:
+  * default precision (fp64, the reference's): the same sweep count as the
+    reference / oracle at every step, positions within 1e-10 of the
+    bounding-box diagonal (measured: about 1e-14);
+  * precision="mixed" (fp32 per-slot arithmetic): within 1e-5 of the
+    diagonal and 1e-5 relative tip displacement over the 20x2x2 cantilever's
+    300 steps, the bar the solver is specified to (longer trajectories drift
+    further, see test_mixed_precision_drift_is_bounded).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from warpvbd_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FP64_TOL = 1e-10   # x bbox diagonal
+MIXED_TOL = 1e-5   # x bbox diagonal, and relative tip displacement
+
+
+def _diag(X):
+    return float(np.linalg.norm(X.max(0) - X.min(0)))
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return np.load(os.path.join(HERE, "golden", "ref_trajectories.npz"))
+
+
+@pytest.fixture(scope="module")
+def long():
+    return np.load(os.path.join(HERE, "golden", "oracle_long.npz"))
+
+
+def _ref_case(ref, name):
+    p = json.loads(str(ref[f"{name}/params"]))
+    X = ref[f"{name}/vertices"]
+    T = ref[f"{name}/tets"]
+    act = ref[f"{name}/active"]
+    n = T.shape[0]
+    kw = dict(initial_positions=X, elements=T, densities=np.full(n, p["rho"]),
+              youngs_modulus=np.full(n, p["E"]), poissons_ratio=np.full(n, p["nu"]),
+              active_mask=act, damping_coefficient=p["kd"], dx_tol=p["tol"],
+              max_iter=p["max_iter"])
+    return p, kw
+
+
+CASES = ["cantilever20_snh", "cantilever20_stvk", "cantilever20_damped",
+         "cantilever20_maxiter3", "massspring5_6"]
+
+
+@pytest.mark.parametrize("mode", ["auto", "block", "persist", "graph"])
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_reference_trajectory(ref, name, mode, capsys):
+    from warpvbd_b200 import VBDSolver
+    p, kw = _ref_case(ref, name)
+    g = VBDSolver(**kw, material=p["material"], mode=mode)
+    assert g.precision == "fp64"
+    # tables exposed to callers, as the reference built them
+    assert np.array_equal(g.color_groups, ref[f"{name}/color_groups"])
+    assert np.array_equal(g.adj_v2e, ref[f"{name}/adj_v2e"])
+    D = _diag(kw["initial_positions"])
+    rec = set(ref[f"{name}/rec_steps"].tolist())
+    pos = ref[f"{name}/positions"]
+    sweeps = ref[f"{name}/sweeps"]
+    warned = ref[f"{name}/warned"]
+    final_dx = ref[f"{name}/final_dx"] if f"{name}/final_dx" in ref.files else None
+    worst, j = 0.0, 0
+    for k in range(1, len(sweeps) + 1):
+        x = g.step(g.old_positions, p["dt"]).numpy()
+        out = capsys.readouterr().out
+        assert g.last_iterations == sweeps[k - 1], (k, g.last_iterations, sweeps[k - 1])
+        assert ("did not converge" in out) == bool(warned[k - 1]), (k, out)
+        if warned[k - 1] and final_dx is not None:
+            # the value the reference's warning prints: the last sweep's
+            # largest |dx| component
+            mine = float(out.split("Final dx max:")[1].split()[0])
+            assert abs(mine - final_dx[k - 1]) <= 1e-9 * final_dx[k - 1], (k, mine, final_dx)
+        if k in rec:
+            worst = max(worst, np.abs(x - pos[j]).max() / D)
+            j += 1
+    print(f"{name} {mode}: {len(sweeps)} steps, max |x - x_ref| = {worst:.2e} of the diagonal")
+    assert worst < FP64_TOL, worst
+
+
+@pytest.mark.parametrize("mode", ["block", "persist", "graph"])
+@pytest.mark.parametrize("name", ["cantilever20_snh", "cantilever20_stvk"])
+def test_mixed_precision_within_spec_of_reference(ref, name, mode):
+    """precision="mixed" against the reference's own trajectory: 1e-5 of
+    the diagonal per vertex and 1e-5 relative tip displacement."""
+    from warpvbd_b200 import VBDSolver
+    p, kw = _ref_case(ref, name)
+    g = VBDSolver(**kw, material=p["material"], mode=mode, precision="mixed")
+    X = kw["initial_positions"]
+    D = _diag(X)
+    tip = np.nonzero(kw["active_mask"] & (X[:, 0] > X[:, 0].max() - 1e-3))[0]
+    rec = ref[f"{name}/rec_steps"].tolist()
+    pos = ref[f"{name}/positions"]
+    sweeps = ref[f"{name}/sweeps"]
+    worst, j, flips = 0.0, 0, 0
+    for k in range(1, len(sweeps) + 1):
+        x = g.step(g.old_positions, p["dt"]).numpy()
+        flips += int(g.last_iterations != sweeps[k - 1])
+        if k in rec:
+            worst = max(worst, np.abs(x - pos[j]).max() / D)
+            j += 1
+    dg = (x[tip] - X[tip]).mean(0)
+    dr = (pos[-1][tip] - X[tip]).mean(0)
+    rel = np.linalg.norm(dg - dr) / np.linalg.norm(dr)
+    print(f"mixed {name} {mode}: worst {worst:.2e}, tip {rel:.2e}, {flips} sweep-count flips")
+    assert worst < MIXED_TOL, worst
+    assert rel < MIXED_TOL, rel
+
+
+def _compare_long(long, key, s, solver_factory, material="snh"):
+    g = solver_factory(s)
+    sweeps = long[f"{key}/sweeps"]
+    tip = long[f"{key}/tip"]
+    sub = long[f"{key}/sub"]
+    disp = long[f"{key}/disp"].astype(np.float64)
+    D = _diag(s.vertices)
+    bad_sweeps, tip_worst = 0, 0.0
+    for k in range(len(sweeps)):
+        g.step(g.old_positions, 1e-3)
+        bad_sweeps += int(g.last_iterations != sweeps[k])
+        if (k + 1) % 25 == 0 or k + 1 == len(sweeps):
+            x = g.old_positions.numpy()
+            d = (x[s.tip] - s.vertices[s.tip]).mean(0)
+            tip_worst = max(tip_worst, np.linalg.norm(d - tip[k]) / np.linalg.norm(tip[k]))
+    err = np.abs((x[sub] - s.vertices[sub]) - disp).max() / D
+    return bad_sweeps, tip_worst, err
+
+
+def test_fp64_mass_spring_1000_steps_matches_oracle(long):
+    """Mass-spring (11^3 cube on a 1x1x20 column), 1000 steps."""
+    from warpvbd_b200 import VBDSolver
+    s = scenes.mass_spring(11, 20)
+    bad, tip, err = _compare_long(long, "c3", s, lambda s: VBDSolver(
+        **s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000, tune=True))
+    print(f"c3: sweep mismatches {bad}, tip {tip:.2e}, positions {err:.2e}")
+    assert bad == 0
+    assert tip < 1e-9
+    assert err < 1e-7  # float32 storage of the fixture's displacements
+
+
+@pytest.mark.parametrize("material,steps", [("snh", 300), ("stvk", 100)])
+def test_fp64_cantilever_160_matches_oracle(long, material, steps):
+    """160x16x16 cantilever (46,529 vertices), tuned persistent launch."""
+    from warpvbd_b200 import VBDSolver
+    s = scenes.cantilever(160)
+    key = f"c160_{material}"
+    assert len(long[f"{key}/sweeps"]) == steps
+    bad, tip, err = _compare_long(long, key, s, lambda s: VBDSolver(
+        **s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000,
+        material=material, tune=True))
+    print(f"{key}: sweep mismatches {bad}, tip {tip:.2e}, positions {err:.2e}")
+    assert bad == 0
+    assert tip < 1e-9
+    assert err < 1e-7
+
+
+def test_fp64_batch_256_envs_300_steps(long):
+    """The 256-environment batch for 300 steps with the tuned tiered launch:
+    the 32 environments of the fixture against the FP64 oracle (same sweep
+    count every step, positions), and all 256 against a second launch shape
+    (one block per environment, other lanes per vertex): every environment's
+    trajectory is the same to rounding."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(256, seed=0)
+    a = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, tune=True)
+    b = BatchedVBDSolver(envs, dx_tol=1e-7, max_iter=1000, tpv=2, block_threads=256, cluster=1)
+    ids = long["c4/envs"]
+    sweeps = long["c4/sweeps"]
+    tips = long["c4/tip"]
+    its_a = np.zeros((300, 256), np.int32)
+    flips = 0
+    for k in range(300):
+        its_a[k] = a.step(1e-3)
+        flips += int((b.step(1e-3) != its_a[k]).sum())
+    xa, xb = a.positions(), b.positions()
+    assert flips == 0
+    assert np.array_equal(its_a[:, ids], sweeps.T.astype(np.int32))
+    subs, offs = long["c4/sub"], long["c4/sub_offsets"]
+    disp = long["c4/disp"].astype(np.float64)
+    worst_o, worst_ab = 0.0, 0.0
+    for e in range(256):
+        env = envs[e]
+        sl = a.env_slice(e)
+        D = _diag(env.vertices)
+        worst_ab = max(worst_ab, np.abs(xa[sl] - xb[sl]).max() / D)
+    for j, e in enumerate(ids):
+        env = envs[e]
+        x = xa[a.env_slice(e)]
+        d = (x[env.tip] - env.vertices[env.tip]).mean(0)
+        t = tips[j, -1]
+        assert np.linalg.norm(d - t) / np.linalg.norm(t) < 1e-9, e
+        sub = subs[offs[j]:offs[j + 1]]
+        worst_o = max(worst_o, np.abs((x[sub] - env.vertices[sub]) - disp[offs[j]:offs[j + 1]])
+                      .max() / _diag(env.vertices))
+    print(f"batch: 32 envs vs oracle {worst_o:.2e}, 256 envs shape A vs B {worst_ab:.2e}")
+    assert worst_o < 1e-7
+    assert worst_ab < FP64_TOL
+
+
+def test_mixed_precision_drift_is_bounded(long):
+    """precision="mixed" over the long trajectories: fp32 rounding of the
+    per-slot terms shifts the stopping sweep of some steps (the flips), and
+    each shift moves the state by up to the tolerance over (1 - per-sweep
+    contraction); the drift stays within the bounds measured on B200
+    (mass-spring 1000 steps 2e-6, cantilever 160 SNH 300 steps 1.6e-5, of
+    the diagonal), with margin."""
+    from warpvbd_b200 import VBDSolver
+    s = scenes.mass_spring(11, 20)
+    bad, tip, err = _compare_long(long, "c3", s, lambda s: VBDSolver(
+        **s.solver_kwargs(), damping_coefficient=0.0, dx_tol=1e-7, max_iter=1000,
+        precision="mixed", tune=True))
+    print(f"mixed c3: flips {bad}, tip {tip:.2e}, positions {err:.2e}")
+    assert err < 2e-5

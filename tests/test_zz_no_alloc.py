@@ -60,6 +60,13 @@ def test_step_noalloc_matches_step_twice_in_a_row():
             assert np.abs(xn - xr).max() < POS_TOL * diag, (call, np.abs(xn - xr).max())
             assert it_na.value == it_ref.value, (call, it_na.value, it_ref.value)
             assert not np.array_equal(xn, s.vertices)   # the step moved the beam
+            # the step's own kernel time and launch count: begin and end, and
+            # per sweep one launch per colour plus the reduction and the check
+            info = _lib.VBDInfo()
+            _lib.check(L.vbd_get_info(na, ctypes.byref(info)))
+            assert info.last_step_launches == 2 + it_na.value * (info.n_colors + 2), \
+                (info.last_step_launches, it_na.value, info.n_colors)
+            assert info.last_step_kernel_ms > 0.0
     finally:
         L.vbd_destroy(ref)
         L.vbd_destroy(na)

@@ -44,6 +44,18 @@ ORDER_INDEX = 0x1000
 STRICT_SPD = 0x2000
 TIERED = 0x4000
 CLUSTER_SHIFT = 16
+MAX_CLUSTER = 16
+
+
+def cluster_flags(cluster):
+    """The flag bits of a block-mode cluster size: 0 (automatic) or 1 to 16
+    thread blocks per cluster; anything else raises ValueError (the field
+    is 5 bits wide, so a larger value must not be shifted in)."""
+    c = int(cluster)
+    if c != cluster or not 0 <= c <= MAX_CLUSTER:
+        raise ValueError(f"cluster must be an integer from 0 (automatic) to {MAX_CLUSTER}, "
+                         f"got {cluster!r}")
+    return c << CLUSTER_SHIFT
 
 MODE_PERSIST = 0x400
 MODES = {"auto": MODE_AUTO, "block": MODE_BLOCK, "graph": MODE_GRAPH, "hostloop": MODE_HOSTLOOP,
@@ -95,6 +107,7 @@ SIGNATURES = {
                                            ctypes.c_int, _ip, _d]),
     "vbd_sync": (ctypes.c_int, [_vp]),
     "vbd_get_iterations": (ctypes.c_int, [_vp, _ip]),
+    "vbd_get_final_dx": (ctypes.c_int, [_vp, _d]),
     "vbd_get_positions": (ctypes.c_int, [_vp, _d]),
     "vbd_set_positions": (ctypes.c_int, [_vp, _d]),
     "vbd_get_velocities": (ctypes.c_int, [_vp, _d]),

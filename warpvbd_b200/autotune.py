@@ -199,7 +199,7 @@ def _fits_block(n_vertices, precision):
     return n_vertices * STATE_BYTES[precision] <= BLOCK_SMEM_LIMIT
 
 
-def tune_single(solver_kwargs, *, material="snh", precision="mixed", device="cuda",
+def tune_single(solver_kwargs, *, material="snh", precision="fp64", device="cuda",
                 damping_coefficient=0.0, dt=1e-3, dx_tol=1e-7, max_iter=1000, steps=4, warmup=2,
                 spaces=None, cache_path=None, refresh=False, verbose=False):
     """Fastest launch shape for one mesh: a dict of VBDSolver keyword
@@ -251,7 +251,7 @@ def tune_single(solver_kwargs, *, material="snh", precision="mixed", device="cud
     return cfg
 
 
-def tune_batched(envs, *, material="snh", precision="mixed", device="cuda", dt=1e-3,
+def tune_batched(envs, *, material="snh", precision="fp64", device="cuda", dt=1e-3,
                  dx_tol=1e-7, max_iter=1000, steps=12, warmup=4, spaces=None, cache_path=None,
                  refresh=False, verbose=False, warm=None):
     """Fastest launch shape for a batch of environments: a dict of
@@ -321,7 +321,7 @@ def _kwargs(cfg):
     return out
 
 
-def cached_single(solver_kwargs, *, material="snh", precision="mixed", device="cuda",
+def cached_single(solver_kwargs, *, material="snh", precision="fp64", device="cuda",
                   cache_path=None):
     """The cached configuration of a mesh (user cache, then the committed
     table), or None: nothing is measured."""
@@ -331,7 +331,7 @@ def cached_single(solver_kwargs, *, material="snh", precision="mixed", device="c
                   cache_path)
 
 
-def cached_batched(envs, *, material="snh", precision="mixed", device="cuda", cache_path=None,
+def cached_batched(envs, *, material="snh", precision="fp64", device="cuda", cache_path=None,
                    warm=False):
     """The cached configuration of a batch (`warm`: tuned with the learned
     warm start on), or None: nothing is measured."""
@@ -364,7 +364,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument("workloads", nargs="+")
     ap.add_argument("--out", default=None, help="cache file (default: the user cache)")
-    ap.add_argument("--precision", default="mixed")
+    ap.add_argument("--precision", default="fp64")
     ap.add_argument("--refresh", action="store_true")
     ap.add_argument("--warm", action="store_true",
                     help="batched workloads: tune with the committed warm-start model on")

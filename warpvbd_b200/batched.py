@@ -23,7 +23,7 @@ class BatchedVBDSolver:
     with the ``VBDSolver`` argument names."""
 
     def __init__(self, envs, damping_coefficient=0.0, gravity=(0.0, 0.0, -9.81), dx_tol=1e-7,
-                 max_iter=1000, device="cuda", *, material="snh", precision="mixed",
+                 max_iter=1000, device="cuda", *, material="snh", precision="fp64",
                  tpv=0, block_threads=0, cluster=0, order_index=False, tiered=False,
                  tune=False):
         """``cluster``: blocks per thread-block cluster (0 = automatic); an
@@ -68,7 +68,7 @@ class BatchedVBDSolver:
         flags = {"snh": _lib.MATERIAL_SNH, "stvk": _lib.MATERIAL_STVK}[material]
         flags |= _lib.PRECISIONS[precision]
         flags |= _lib.MODE_BLOCK
-        flags |= int(cluster) << _lib.CLUSTER_SHIFT
+        flags |= _lib.cluster_flags(cluster)
         if order_index:
             flags |= _lib.ORDER_INDEX
         if tiered:

@@ -84,6 +84,51 @@ __device__ __forceinline__ void slot_accumulate(Real d0x, Real d0y, Real d0z, Re
   const Real bz = -(q0.z + q1.z + q2.z);
   const Real p0 = q0.w, p1 = q1.w;
   const Real bb = bx * bx + by * by + bz * bz;
+  if (MAT == kSNH && sizeof(Real) == 8) {
+    // fp64: the reference's own form (vbd_solver.py:111-114, 118-123)
+    //   P b = mu' (1 - 1/(Ic+1)) F b + lambda' (J - alpha) cof(F) b
+    // with lambda' (J - alpha) = lambda' (J - 1) - 3/4 mu'.  The difference
+    // J - 1 cancels at small strain, as the reference's J - alpha does; in
+    // double precision that costs ~1e-16 / strain relative, far below the
+    // solver's tolerance, and it needs fewer operations and live values than
+    // the cancellation-free form the fp32 path uses below.
+    const Real F00 = Real(1) + G00, F11 = Real(1) + G11, F22 = Real(1) + G22;
+    const Real Fbx = F00 * bx + G01 * by + G02 * bz;
+    const Real Fby = G10 * bx + F11 * by + G12 * bz;
+    const Real Fbz = G20 * bx + G21 * by + F22 * bz;
+    const Real Ic = F00 * F00 + G01 * G01 + G02 * G02 + G10 * G10 + F11 * F11 + G12 * G12 +
+                    G20 * G20 + G21 * G21 + F22 * F22;
+    // cof(F) row by row: J from row 0, cof(F) b from all three
+    Real c0 = F11 * F22 - G12 * G21, c1 = G12 * G20 - G10 * F22, c2 = G10 * G21 - F11 * G20;
+    const Real J = F00 * c0 + G01 * c1 + G02 * c2;
+    const Real Cbx = c0 * bx + c1 * by + c2 * bz;
+    c0 = G21 * G02 - F22 * G01;
+    c1 = F22 * F00 - G20 * G02;
+    c2 = G20 * G01 - G21 * F00;
+    const Real Cby = c0 * bx + c1 * by + c2 * bz;
+    c0 = G01 * G12 - G02 * F11;
+    c1 = G02 * G10 - F00 * G12;
+    c2 = F00 * F11 - G01 * G10;
+    const Real Cbz = c0 * bx + c1 * by + c2 * bz;
+    const Real p0 = q0.w, p1 = q1.w;
+    const Real inv = Real(1) / (Ic + Real(1));
+    const Real a = p0 * (Real(1) - inv);
+    const Real kJ = p1 * (J - Real(1)) - Real(0.75) * p0;
+    g[0] += a * Fbx + kJ * Cbx;
+    g[1] += a * Fby + kJ * Cby;
+    g[2] += a * Fbz + kJ * Cbz;
+    const Real hF = Real(2) * p0 * inv * inv;
+    const Real hI = a * bb;
+    const Real Fx = hF * Fbx, Fy = hF * Fby, Fz = hF * Fbz;
+    const Real Cx = p1 * Cbx, Cy = p1 * Cby, Cz = p1 * Cbz;
+    h[0] += Fx * Fbx + Cx * Cbx + hI;
+    h[1] += Fx * Fby + Cx * Cby;
+    h[2] += Fx * Fbz + Cx * Cbz;
+    h[3] += Fy * Fby + Cy * Cby + hI;
+    h[4] += Fy * Fbz + Cy * Cbz;
+    h[5] += Fz * Fbz + Cz * Cbz + hI;
+    return;
+  }
   const Real Gbx = G00 * bx + G01 * by + G02 * bz;
   const Real Gby = G10 * bx + G11 * by + G12 * bz;
   const Real Gbz = G20 * bx + G21 * by + G22 * bz;
@@ -308,7 +353,8 @@ template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
 __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const ColorInfo& ci,
                                               int q, int lane, const State& st,
                                               const StepConst& sc, unsigned long long& cmax,
-                                              unsigned& stat, const real4<Real>* tab) {
+                                              unsigned& stat, const real4<Real>* tab,
+                                              unsigned long long* dxrec = nullptr) {
   using R4 = real4<Real>;
   using S4 = real4<SReal>;
   constexpr int CPW = 32 / TPV;
@@ -428,6 +474,11 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
     if (!isfinite(c)) stat |= kStatNonFinite;
     const unsigned long long cb = conv_bits(c);
     cmax = cb > cmax ? cb : cmax;
+    // the last sweep allowed: its largest |dx| component, for the
+    // non-convergence report
+    if (dxrec)
+      atomicMax(dxrec, conv_bits(fmax(fabs(double(dx[0])),
+                                      fmax(fabs(double(dx[1])), fabs(double(dx[2]))))));
   }
 }
 

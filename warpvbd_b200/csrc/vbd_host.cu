@@ -488,6 +488,10 @@ struct vbd_solver {
   int fmt = kFmtIdx32;
   DevBuf<int> d_valence, d_map, d_iters;
   DevBuf<unsigned> d_status;
+  // per env: largest |dx| component of the last allowed sweep (DevMesh::dxmax)
+  DevBuf<unsigned long long> d_dxmax;
+  unsigned long long* h_dxmax = nullptr;  // pinned
+  std::vector<double> final_dx;           // per env, of the last step; NaN if it converged
   DevBuf<unsigned char> d_u, d_ut, d_up, d_vel;
   DevBuf<double> d_X, d_io, d_tol;
   DevBuf<StepParams> d_params;
@@ -587,6 +591,7 @@ struct vbd_solver {
     m.vel = d_vel.p;
     m.iters = d_iters.p;
     m.status = d_status.p;
+    m.dxmax = d_dxmax.p;
     m.n_env = n_env;
     m.n_vertices = V;
     return m;
@@ -617,6 +622,7 @@ void free_solver(vbd_solver* s) {
   s->d_map.release();
   s->d_iters.release();
   s->d_status.release();
+  s->d_dxmax.release();
   s->d_u.release();
   s->d_ut.release();
   s->d_up.release();
@@ -650,6 +656,7 @@ void free_solver(vbd_solver* s) {
   s->d_pparts.release();
   if (s->h_iters) cudaFreeHost(s->h_iters);
   if (s->h_status) cudaFreeHost(s->h_status);
+  if (s->h_dxmax) cudaFreeHost(s->h_dxmax);
   if (s->h_params) cudaFreeHost(s->h_params);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   if (s->h_ws_err) cudaFreeHost(s->h_ws_err);
@@ -903,7 +910,9 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   s->mode = mode;
   const bool block_mode = mode == VBD_MODE_BLOCK;
   const int cl = (flags >> VBD_CLUSTER_SHIFT) & 0x1F;
-  if (cl > 16) {
+  // the cluster field is 5 bits wide and nothing lies above it: a set bit
+  // there is a cluster size that did not fit (or a negative one)
+  if (cl > 16 || (static_cast<unsigned>(flags) >> (VBD_CLUSTER_SHIFT + 5)) != 0u) {
     delete s;
     return fail(VBD_ERR_INVALID_ARG, "cluster size must be 0 (automatic) or 1 to 16");
   }
@@ -1040,6 +1049,7 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   if (!err && bad(s->d_tol.alloc(s->n_env), "tol")) err = 1;
   if (!err && bad(s->d_iters.alloc(s->n_env), "iters")) err = 1;
   if (!err && bad(s->d_status.alloc(s->n_env), "status")) err = 1;
+  if (!err && bad(s->d_dxmax.alloc(s->n_env), "dxmax")) err = 1;
   if (!err && bad(s->d_params.alloc(1), "params")) err = 1;
   if (!err && bad(s->d_ctl.alloc(1), "ctl")) err = 1;
   if (!err && mode == VBD_MODE_PERSIST) {
@@ -1088,6 +1098,7 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     }
     cudaMemsetAsync(s->d_iters.p, 0, sizeof(int) * s->n_env, st);
     cudaMemsetAsync(s->d_status.p, 0, sizeof(unsigned) * s->n_env, st);
+    cudaMemsetAsync(s->d_dxmax.p, 0, sizeof(unsigned long long) * s->n_env, st);
   }
   if (!err && bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_iters), sizeof(int) * s->n_env),
                   "pinned"))
@@ -1096,6 +1107,11 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
       bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_status), sizeof(unsigned) * s->n_env),
           "pinned"))
     err = 1;
+  if (!err && bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_dxmax),
+                                 sizeof(unsigned long long) * s->n_env),
+                  "pinned"))
+    err = 1;
+  s->final_dx.assign(s->n_env, std::nan(""));
   if (!err && bad(cudaMallocHost(reinterpret_cast<void**>(&s->h_params), sizeof(StepParams)),
                   "pinned"))
     err = 1;
@@ -1358,13 +1374,15 @@ int ws_error_status(vbd_solver* s) {
   return fail(VBD_ERR_TIMEOUT, "warm-start inference: a tensor-core wait timed out");
 }
 
-int finish(vbd_solver* s, int* iters_out) {
+// warm_step: the step ran the learned warm start (its inference may have
+// recorded a timeout in d_ws_err)
+int finish(vbd_solver* s, int* iters_out, bool warm_step) {
   cudaStream_t st = s->stream;
   CUDA_TRY(cudaMemcpyAsync(s->h_iters, s->d_iters.p, sizeof(int) * s->n_env,
                            cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaMemcpyAsync(s->h_status, s->d_status.p, sizeof(unsigned) * s->n_env,
                            cudaMemcpyDeviceToHost, st));
-  if (s->warm && s->h_ws_err)
+  if (warm_step && s->h_ws_err)
     CUDA_TRY(cudaMemcpyAsync(s->h_ws_err, s->d_ws_err.p, sizeof(unsigned),
                              cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -1378,8 +1396,25 @@ int finish(vbd_solver* s, int* iters_out) {
                          ? s->launches_pending
                          : 2 + s->h_iters[0] * ((int)s->L.color.size() + 1);
   if (iters_out) std::memcpy(iters_out, s->h_iters, sizeof(int) * s->n_env);
+  // environments that used every allowed sweep recorded the largest |dx|
+  // component of the last one: read it, then clear the words for the next
+  // step that reaches its cap (the stream is idle here)
+  bool capped = false;
+  for (int e = 0; e < s->n_env; ++e) capped |= (s->h_status[e] & kStatIterCap) != 0;
+  std::fill(s->final_dx.begin(), s->final_dx.end(), std::nan(""));
+  if (capped) {
+    CUDA_TRY(cudaMemcpy(s->h_dxmax, s->d_dxmax.p, sizeof(unsigned long long) * s->n_env,
+                        cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemset(s->d_dxmax.p, 0, sizeof(unsigned long long) * s->n_env));
+    for (int e = 0; e < s->n_env; ++e)
+      if (s->h_status[e] & kStatIterCap) {
+        double v;
+        std::memcpy(&v, &s->h_dxmax[e], sizeof v);
+        s->final_dx[e] = v;
+      }
+  }
   s->last_status = status_from_bits(s, s->h_status);
-  if (s->last_status >= 0) {
+  if (s->last_status >= 0 && warm_step) {
     const int ws = ws_error_status(s);
     if (ws != VBD_OK) s->last_status = ws;
   }
@@ -1514,7 +1549,7 @@ int vbd_get_trace(vbd_solver* s, unsigned long long* records, int cap, int* coun
   if (!s || !count) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
   DeviceGuard dg(s->device);
   if (s->pending) {
-    const int rc = finish(s, nullptr);
+    const int rc = finish(s, nullptr, s->warm);
     if (rc < 0) return rc;
   }
   if (!records) {
@@ -1547,7 +1582,7 @@ int vbd_step(vbd_solver* s, double dt, double tol, int max_iter, int* iterations
   int rc = enqueue_step(s, dt, tol, nullptr, max_iter);
   if (rc != VBD_OK) return rc;
   if (!iterations_out) return VBD_OK;
-  return finish(s, iterations_out);
+  return finish(s, iterations_out, s->warm);
 }
 
 int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per_env,
@@ -1560,7 +1595,7 @@ int vbd_step_batched(vbd_solver* s, double dt, double tol, const double* tol_per
   int rc = enqueue_step(s, dt, tol, tol_per_env, max_iter);
   if (rc != VBD_OK) return rc;
   if (!iterations_out) return VBD_OK;
-  return finish(s, iterations_out);
+  return finish(s, iterations_out, s->warm);
 }
 
 static int exchange(vbd_solver* s, const double* in, double* out, bool positions);
@@ -1582,7 +1617,7 @@ int vbd_step_batched_to(vbd_solver* s, double dt, double tol, const double* tol_
   int rc = enqueue_step(s, dt, tol, tol_per_env, max_iter);
   s->host_out = nullptr;
   if (rc != VBD_OK) return rc;
-  rc = finish(s, iterations_out);
+  rc = finish(s, iterations_out, s->warm);
   if (rc < 0 || dptr) return rc;
   const int rc2 = exchange(s, nullptr, positions_out, true);
   return rc2 != VBD_OK ? rc2 : rc;
@@ -1596,17 +1631,28 @@ int vbd_sync(vbd_solver* s) {
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return s->last_status;
   }
-  return finish(s, nullptr);
+  return finish(s, nullptr, s->warm);
 }
 
 int vbd_get_iterations(vbd_solver* s, int* iterations_out) {
   if (!s || !iterations_out) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
   DeviceGuard dg(s->device);
   if (s->pending) {
-    int rc = finish(s, iterations_out);
+    int rc = finish(s, iterations_out, s->warm);
     return rc < 0 ? rc : VBD_OK;
   }
   std::memcpy(iterations_out, s->h_iters, sizeof(int) * s->n_env);
+  return VBD_OK;
+}
+
+int vbd_get_final_dx(vbd_solver* s, double* final_dx_out) {
+  if (!s || !final_dx_out) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
+  DeviceGuard dg(s->device);
+  if (s->pending) {
+    const int rc = finish(s, nullptr, s->warm);
+    if (rc < 0) return rc;
+  }
+  std::memcpy(final_dx_out, s->final_dx.data(), sizeof(double) * s->n_env);
   return VBD_OK;
 }
 
@@ -1747,7 +1793,7 @@ int vbd_incremental_potential(vbd_solver* s, double dt, const double* positions,
   DeviceGuard dg(s->device);
   cudaStream_t st = s->stream;
   if (s->pending) {
-    const int rc = finish(s, nullptr);
+    const int rc = finish(s, nullptr, s->warm);
     if (rc < 0) return rc;
   }
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -1793,7 +1839,7 @@ int vbd_get_env_status(vbd_solver* s, uint32_t* status_out) {
   if (!s || !status_out) return fail(VBD_ERR_INVALID_ARG, "NULL argument");
   DeviceGuard dg(s->device);
   if (s->pending) {
-    const int rc = finish(s, nullptr);
+    const int rc = finish(s, nullptr, s->warm);
     if (rc < 0) return rc;
   }
   std::memcpy(status_out, s->h_status, sizeof(uint32_t) * s->n_env);
@@ -1838,7 +1884,10 @@ int vbd_mlp_adam(float* params, const float* grad, float* m, float* v, int n, fl
 // Allocation-free step (see vbd_noalloc.cu for who needs it and the limits of
 // its static scratch).  Runs the grid-mode colour sweep one sweep at a time
 // from the host; every buffer it touches either belongs to the solver (made
-// by vbd_create) or is the static scratch.
+// by vbd_create) or is the static scratch.  It always takes a plain step: on
+// a solver with the learned warm start enabled the prediction is not used
+// (its feature and inference buffers are allocated on first use).  The step's
+// kernel time and launch count are recorded for vbd_get_info like vbd_step's.
 int vbd_step_noalloc(vbd_solver* s, double dt, double tol, int max_iter, int* iterations_out) {
   if (!s) return fail(VBD_ERR_INVALID_ARG, "NULL solver");
   if (s->n_env != 1)
@@ -1846,6 +1895,10 @@ int vbd_step_noalloc(vbd_solver* s, double dt, double tol, int max_iter, int* it
   if (!(dt > 0.0) || !std::isfinite(dt)) return fail(VBD_ERR_INVALID_ARG, "dt must be > 0");
   if (max_iter < 1) return fail(VBD_ERR_INVALID_ARG, "max_iter must be >= 1");
   DeviceGuard dg(s->device);
+  if (s->pending) {  // an enqueued step: collect its results first
+    const int rc = finish(s, nullptr, s->warm);
+    if (rc < 0) return rc;
+  }
   const EnvInfo& e = s->L.env[0];
   int total = 0;  // convergence partials one sweep writes (one per thread block)
   for (int c = e.cbase; c < e.cbase + e.ncolors; ++c) {
@@ -1875,7 +1928,9 @@ int vbd_step_noalloc(vbd_solver* s, double dt, double tol, int max_iter, int* it
   const DevMesh m = s->mesh();
   // from pageable memory: the copy has read `p` when the call returns
   CUDA_TRY(cudaMemcpyAsync(dp, &p, sizeof p, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaEventRecord(s->ev_k0, st));
   CUDA_TRY(launch_begin(s->state64, m, dp, ctl, st));  // also zeroes the loop control
+  int launches = 2;  // begin, end
   LoopControl hc{};
   for (int it = 0; it < max_iter; ++it) {
     int off = 0;
@@ -1885,16 +1940,21 @@ int vbd_step_noalloc(vbd_solver* s, double dt, double tol, int max_iter, int* it
       CUDA_TRY(launch_noalloc_color(s->prec, s->material, s->tpv, m, c, blocks, dp, ctl,
                                     partial + off, st));
       off += blocks;
+      launches += blocks > 0 ? 1 : 0;
     }
     CUDA_TRY(launch_noalloc_reduce(partial, off, ctl, st));
     CUDA_TRY(launch_check(ctl, dp, 0ull, 0, st));
+    launches += 2;
     CUDA_TRY(cudaMemcpyAsync(&hc, ctl, sizeof hc, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     if (hc.status & 0x80000000u) break;
   }
   CUDA_TRY(launch_end(s->state64, m, dp, ctl, st));
+  CUDA_TRY(cudaEventRecord(s->ev_k1, st));
+  s->launches_pending = launches;
+  s->trace_pending = 0;
   s->pending = true;
-  return finish(s, iterations_out);
+  return finish(s, iterations_out, false);
 }
 
 }  // extern "C"

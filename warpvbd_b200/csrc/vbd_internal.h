@@ -109,6 +109,11 @@ struct DevMesh {
   void* vel;
   int* iters;           // per env
   unsigned* status;     // per env
+  // per env: the largest |dx| component of the sweep numbered max_iter (the
+  // last one allowed), as the bits of a non-negative double; written only on
+  // that sweep, read when the step hit max_iter (the reference prints it in
+  // its non-convergence warning, vbd_solver.py:581-582)
+  unsigned long long* dxmax;
   int n_env;
   int n_vertices;
   int fmt;  // RecordFormat

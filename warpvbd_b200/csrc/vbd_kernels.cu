@@ -95,16 +95,18 @@ __device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, co
                                           double tol, unsigned& stat, bool& converged,
                                           unsigned long long* s_red,
                                           unsigned long long (*s_conv)[kMaxGroup],
-                                          int* s_done, const real4<Real>* tab) {
+                                          int* s_done, const real4<Real>* tab,
+                                          unsigned long long* dxw) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   int it = 0;
   for (;;) {
     unsigned long long cmax = 0ull;
+    unsigned long long* dxrec = it + 1 == max_iter ? dxw : nullptr;
     for (int c = 0; c < e.ncolors; ++c) {
       const ColorInfo ci = m.color[e.cbase + c];
       for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
         process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, su, sc, cmax, stat,
-                                                  tab);
+                                                  tab, dxrec);
       group_sync<GROUP>(g);
     }
     ++it;
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, su, rank, g, sc, p.max_iter, tol,
                                                         stat, converged, s_red, s_conv, &s_done,
-                                                        tab);
+                                                        tab, m.dxmax + env);
   } else {
     __syncthreads();
     if (p.warm && m.ws_pred) {
@@ -347,7 +349,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, p.max_iter, tol,
                                                         stat, converged, s_red, s_conv, &s_done,
-                                                        tab);
+                                                        tab, m.dxmax + env);
   }
   // velocity update and write-back, vertices split over the group
   for (int i = rank + g * threadIdx.x; i < e.nv; i += g * blockDim.x) {
@@ -422,9 +424,12 @@ __global__ void __launch_bounds__(256) color_kernel(DevMesh m, int color,
   unsigned long long cmax = 0ull;
   unsigned stat = 0u;
   const GlobalState<SReal> state{reinterpret_cast<S4*>(m.u)};
+  // sweeps done so far: check_kernel advances it after every sweep
+  unsigned long long* dxrec = ctl->iter + 1 == pp->max_iter ? m.dxmax : nullptr;
   if (q < ci.chunk_end)
     process_chunk<Real, SReal, TPV, MAT, FMT>(m, 0, ci, q, lane, state, sc, cmax, stat,
-                                              reinterpret_cast<const real4<Real>*>(m.rec_tab));
+                                              reinterpret_cast<const real4<Real>*>(m.rec_tab),
+                                              dxrec);
   cmax = warp_max_u64(cmax);
   const unsigned st = __reduce_or_sync(0xffffffffu, stat);
   if (lane == 0) {

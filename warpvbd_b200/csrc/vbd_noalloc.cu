@@ -59,9 +59,11 @@ __global__ void __launch_bounds__(256) noalloc_color_kernel(DevMesh m, int color
   unsigned long long cmax = 0ull;
   unsigned stat = 0u;
   const GlobalState<SReal> state{reinterpret_cast<S4*>(m.u)};
+  unsigned long long* dxrec = ctl->iter + 1 == pp->max_iter ? m.dxmax : nullptr;
   if (q < ci.chunk_end)
     process_chunk<Real, SReal, TPV, MAT, FMT>(m, 0, ci, q, lane, state, sc, cmax, stat,
-                                              reinterpret_cast<const real4<Real>*>(m.rec_tab));
+                                              reinterpret_cast<const real4<Real>*>(m.rec_tab),
+                                              dxrec);
   cmax = warp_max_u64(cmax);
   const unsigned st = __reduce_or_sync(0xffffffffu, stat);
   if (lane == 0) {

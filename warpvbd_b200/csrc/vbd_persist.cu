@@ -283,6 +283,7 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
   bool conv = false, nan = false;
   for (;;) {
     unsigned long long cmax = 0ull;
+    unsigned long long* dxrec = it + 1 == max_iter ? m.dxmax : nullptr;
     for (int c = 0; c < e.ncolors; ++c) {
       const ColorInfo ci = m.color[e.cbase + c];
       const bool small = is_small(ci.chunk_end - ci.chunk_begin);
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
         for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
              q += span * nwarps)
           process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, cmax,
-                                                    stat, tab);
+                                                    stat, tab, dxrec);
       if (c + 1 == e.ncolors) break;
       const ColorInfo cn = m.color[e.cbase + c + 1];
       if (small && is_small(cn.chunk_end - cn.chunk_begin)) {

@@ -80,10 +80,18 @@ __all__ = ["tet_surface", "write_obj", "tip_positions", "save_tip_csv", "save_ti
 
 
 def save_state(path, positions, velocities, **extra):
-    """Checkpoint of a solver's state (x, v) -- all a VBD step depends on --
-    as a compressed npz (float64 [n, 3] each; `extra` arrays are stored too,
-    e.g. the step count).  Restore with load_state and the solver's
-    set_state(positions=..., velocities=...)."""
+    """Checkpoint of a solver's state (x, v) as a compressed npz (float64
+    [n, 3] each; `extra` arrays are stored too, e.g. the step count).  Restore
+    with load_state and the solver's set_state(positions=..., velocities=...).
+
+    (x, v) is all a plain VBD step depends on, and a restored plain run
+    continues like the uninterrupted one (same sweep counts; positions equal
+    up to the rounding of x - X).  A solver with the learned warm start also
+    feeds the previous step's inertia target to its network, which a fresh
+    solver does not have: after a restore its first step predicts from
+    (x, v) alone and may take another candidate, so a resumed warm-started run
+    agrees with the uninterrupted one to the solver's tolerance (both stop
+    when the update falls below dx_tol), not bit for bit."""
     np.savez_compressed(path, positions=np.asarray(positions, np.float64),
                         velocities=np.asarray(velocities, np.float64),
                         **{k: np.asarray(v) for k, v in extra.items()})

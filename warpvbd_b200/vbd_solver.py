@@ -154,8 +154,14 @@ class VBDSolver:
     Extra keyword arguments (all optional, not in the reference):
       material   "snh" (Stable Neo-Hookean, the reference's active model) or
                  "stvk" (St. Venant-Kirchhoff, the reference's commented model)
-      precision  "mixed" (default: fp64 positions and velocities, fp32 arithmetic),
-                 "fp32" (everything fp32) or "fp64" (everything fp64)
+      precision  "fp64" (default: state and arithmetic in double precision, as in
+                 the reference, whose types are all float64), "mixed" (fp64
+                 positions and velocities, fp32 per-slot arithmetic: faster, but
+                 fp32 rounding moves the stopping sweep of some steps, so long
+                 trajectories drift from the fp64 one; measured up to 1.6e-5 of
+                 the bounding-box diagonal on the 160x16x16 cantilever over 300
+                 steps and 9.6e-5 on the 256-environment batch) or "fp32"
+                 (everything fp32)
       mode       "auto", "block", "graph", "hostloop" or "persist" (see include/vbd_b200.h)
       tpv, block_threads   launch shape (0 = automatic)
       cluster    block mode: spread the mesh over this many thread blocks of one
@@ -172,7 +178,7 @@ class VBDSolver:
     def __init__(self, initial_positions, elements, densities, youngs_modulus, poissons_ratio,
                  damping_coefficient=1.0, active_mask=None, gravity=(0.0, 0.0, -9.81),
                  dx_tol=1e-9, max_iter=100, device="cuda", *, material="snh",
-                 precision="mixed", mode="auto", tpv=0, block_threads=0, cluster=0, coloring=None,
+                 precision="fp64", mode="auto", tpv=0, block_threads=0, cluster=0, coloring=None,
                  strict_spd=False, allow_high_valence=False, verbose=False, order_index=False,
                  tune=False):
         L = _lib.load()
@@ -210,7 +216,7 @@ class VBDSolver:
             flags |= _lib.STRICT_SPD
         if order_index:
             flags |= _lib.ORDER_INDEX
-        flags |= int(cluster) << _lib.CLUSTER_SHIFT
+        flags |= _lib.cluster_flags(cluster)
         self.device = device
         self._dev = _device_index(device)
         h = ctypes.c_void_p()
@@ -381,8 +387,10 @@ class VBDSolver:
                 + _lib.load().vbd_last_error_message().decode(errors="replace"))
         _lib.check(status, "vbd_step")
         if iterations == max_iter:   # the reference's warning condition (vbd_solver.py:581-582)
+            dx = np.full(1, np.nan)
+            _lib.load().vbd_get_final_dx(self._h, _lib.ptr(dx, "d"))
             print("Warning: VBD solver did not converge within the maximum number of "
-                  "iterations.")
+                  f"iterations. Final dx max: {float(dx[0])}")
 
     # ---- learned warm start (see warpvbd_b200.warmstart) --------------------
     def set_warmstart(self, params):
