@@ -79,6 +79,10 @@ typedef struct vbd_solver vbd_solver;
  * at the same time (block_threads threads, shared memory for the largest of
  * them, so several blocks share an SM) */
 #define VBD_TIERED 0x4000
+/* persistent mode: separate the colours of a sweep with grid barriers instead
+ * of the default neighbour-scoped readiness (each block waits only for the
+ * blocks owning vertices that share a tet with its own) */
+#define VBD_PERSIST_GRID_BARRIERS 0x8000
 /* block mode: thread blocks per cluster (1 to 16; 0 = automatic).  An
  * environment much heavier than the others is split over all blocks of one
  * cluster, which share its state through distributed shared memory. */

@@ -1,6 +1,6 @@
-"""Persistent mode (one cooperative launch per step, grid barriers between
-colours) against the per-colour graph mode and the FP64 oracle (GPU tests,
-through the C ABI)."""
+"""Persistent mode (one cooperative launch per step; colours separated by
+neighbour-scoped readiness, or by grid barriers) against the per-colour graph
+mode and the FP64 oracle (GPU tests, through the C ABI)."""
 import numpy as np
 import pytest
 
@@ -46,6 +46,26 @@ def test_persist_matches_graph_mode(n, tpv, threads, precision, bound):
     print(f"persist vs graph, cantilever {n}, tpv {tpv}, {precision}: max diff {worst:.3e} "
           "of the diagonal")
     assert worst < bound, worst
+
+
+@pytest.mark.parametrize("n,tpv,threads,order_index", [
+    (40, 4, 128, False), (80, 16, 128, False), (160, 4, 128, True), (160, 8, 256, False)])
+def test_neighbour_readiness_matches_grid_barriers(n, tpv, threads, order_index):
+    """Waiting only for the neighbouring blocks between colours changes the
+    schedule, not the arithmetic: every vertex still reads the latest values
+    of lower colours and the previous sweep's of higher ones, so positions and
+    sweep counts are bit-identical to the grid-barrier schedule."""
+    s = scenes.cantilever(n)
+    a = _solver(s, "persist", precision="fp64", tpv=tpv, block_threads=threads,
+                order_index=order_index)
+    b = _solver(s, "persist", precision="fp64", tpv=tpv, block_threads=threads,
+                order_index=order_index, persist_sync="grid")
+    assert a.info()["n_blocks"] > 1
+    for _ in range(20 if n >= 160 else 40):
+        xa = a.step(a.old_positions, 1e-3).numpy()
+        xb = b.step(b.old_positions, 1e-3).numpy()
+        assert a.last_iterations == b.last_iterations
+        assert np.array_equal(xa, xb)
 
 
 @pytest.mark.parametrize("n", [40, 80])

@@ -499,6 +499,10 @@ struct vbd_solver {
   DevBuf<PersistCtl> d_pctl;  // persistent mode
   DevBuf<double> d_pparts;    // persistent mode: warm-start energy partial sums
   int persist_blocks = 0;
+  // persistent mode: neighbour-scoped readiness between colours (PersistNbr)
+  DevBuf<int> d_nbr_off, d_nbr_idx;
+  DevBuf<unsigned long long> d_epoch;
+  bool persist_scoped = false;
   PersistLimits wait_limits{1ll << 26, 2000000000ull};  // every grid-barrier wait
   // block-mode work map: (environment, rank, group size) per thread block
   int cluster = 1;           // blocks per cluster = group size of a split environment
@@ -654,6 +658,9 @@ void free_solver(vbd_solver* s) {
   s->d_ctl.release();
   s->d_pctl.release();
   s->d_pparts.release();
+  s->d_nbr_off.release();
+  s->d_nbr_idx.release();
+  s->d_epoch.release();
   if (s->h_iters) cudaFreeHost(s->h_iters);
   if (s->h_status) cudaFreeHost(s->h_status);
   if (s->h_dxmax) cudaFreeHost(s->h_dxmax);
@@ -833,6 +840,62 @@ int upload_plan(vbd_solver* s, const int* iters) {
     s->smem_light = tier_smem(s, s->work2);
   }
   return VBD_OK;
+}
+
+// Neighbour lists of the persistent kernel's readiness waits (PersistNbr):
+// for every block b and colour c, the other blocks that own a solved vertex
+// sharing a tet with one of b's colour-c vertices.  The owner of a vertex
+// follows persist_kernel's assignment exactly: colour c's chunk q goes to
+// block ((q - chunk_begin) / warps per block) mod span, span = every block,
+// or the first nsb blocks for a small colour.
+void build_persist_neighbours(const Layout& L, int tpv, int nwarps, int nb, std::vector<int>& off,
+                              std::vector<int>& idx) {
+  const EnvInfo& e = L.env[0];
+  const int C = e.ncolors, cpw = 32 / tpv;
+  auto is_small = [&](int nch) { return nb > 1 && nch <= kPersistSmallBlocks * nwarps; };
+  int nsb = 1;
+  for (int c = 0; c < C; ++c) {
+    const ColorInfo& ci = L.color[e.cbase + c];
+    const int nch = ci.chunk_end - ci.chunk_begin;
+    if (is_small(nch)) nsb = std::max(nsb, (nch + nwarps - 1) / nwarps);
+  }
+  nsb = std::min(nsb, nb);
+  std::vector<int> owner(e.nsolved, -1);
+  auto for_each_vertex = [&](auto&& f) {
+    for (int c = 0; c < C; ++c) {
+      const ColorInfo& ci = L.color[e.cbase + c];
+      const int span = is_small(ci.chunk_end - ci.chunk_begin) ? nsb : nb;
+      for (int q = ci.chunk_begin; q < ci.chunk_end; ++q) {
+        const int b = ((q - ci.chunk_begin) / nwarps) % span;
+        for (int vi = 0; vi < cpw; ++vi) {
+          const int gv = ci.vbegin + (q - ci.chunk_begin) * cpw + vi;
+          if (gv < ci.vend) f(c, q, vi, gv - e.vbase, b);
+        }
+      }
+    }
+  };
+  for_each_vertex([&](int, int, int, int lv, int b) { owner[lv] = b; });
+  std::vector<std::vector<int>> lists((size_t)nb * C);
+  for_each_vertex([&](int c, int q, int vi, int lv, int b) {
+    const ChunkInfo& ch = L.chunk[q];
+    const int k = L.valence[e.vbase + lv];
+    for (int st = 0; st < ch.steps; ++st)
+      for (int sub = 0; sub < tpv; ++sub) {
+        if (st * tpv + sub >= k) continue;
+        const int4& sl = L.rec_idx[((size_t)ch.block + st) * 32 + vi * tpv + sub];
+        for (int n : {sl.x, sl.y, sl.z})
+          if (n >= 0 && n < e.nsolved && owner[n] >= 0 && owner[n] != b)
+            lists[(size_t)b * C + c].push_back(owner[n]);
+      }
+  });
+  off.assign(1, 0);
+  idx.clear();
+  for (auto& l : lists) {
+    std::sort(l.begin(), l.end());
+    l.erase(std::unique(l.begin(), l.end()), l.end());
+    idx.insert(idx.end(), l.begin(), l.end());
+    off.push_back((int)idx.size());
+  }
 }
 
 int create_impl(const double* X, int V, const int32_t* tets, int T, const double* rho,
@@ -1073,6 +1136,18 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     if (!err && s->persist_blocks < 1) {
       g_last_error = "persistent mode: the kernel does not fit on the device";
       err = 1;
+    }
+    if (!err && s->persist_blocks > 1 && !(flags & VBD_PERSIST_GRID_BARRIERS)) {
+      std::vector<int> off, idx;
+      build_persist_neighbours(s->L, s->tpv, wpb, s->persist_blocks, off, idx);
+      if (idx.empty()) idx.push_back(0);  // a device buffer needs one entry
+      if (bad(s->d_nbr_off.upload(off, st), "persist neighbours") ||
+          bad(s->d_nbr_idx.upload(idx, st), "persist neighbours") ||
+          bad(s->d_epoch.alloc((size_t)s->persist_blocks * kEpochStride), "persist epochs"))
+        err = 1;
+      else
+        s->persist_scoped = true;
+      cudaStreamSynchronize(st);  // off / idx go out of scope
     }
   }
   const size_t sb = s->real4_bytes * (size_t)V;
@@ -1324,9 +1399,11 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
     CUDA_TRY(cudaEventRecord(s->ev_k0, st));
     NvtxRange nk("vbd_step_kernels");
     ++launches;
+    PersistNbr nbr{};
+    if (s->persist_scoped) nbr = PersistNbr{s->d_nbr_off.p, s->d_nbr_idx.p, s->d_epoch.p};
     CUDA_TRY(launch_persist(s->prec, s->material, s->tpv, s->threads, m, s->d_params.p,
                             s->d_pctl.p, s->persist_blocks, s->wait_limits, s->d_pparts.p,
-                            s->persist_smem, st));
+                            s->persist_smem, nbr, st));
   } else if (s->mode == VBD_MODE_GRAPH) {
     rc = build_graph(s);
     if (rc != VBD_OK) return rc;

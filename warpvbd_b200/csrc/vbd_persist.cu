@@ -10,14 +10,16 @@
 //   begin     grid-stride over vertices: ut = u + dt v + dt^2 g, up = u,
 //             active vertices start from ut                      | barrier
 //   sweep     for each colour: warps take the colour's chunks grid-stride
-//             and update their vertices (process_chunk); colours are
-//             separated by a grid barrier, except inside a run of small
-//             colours (at most kSmallBlocks blocks' worth of chunks, e.g.
-//             the 107-vertex colours of a voxel cantilever): those are
-//             done by the first S blocks only (S = blocks the largest small
-//             colour needs), which meet at a barrier among themselves
-//             (__syncthreads when S = 1) while the others go on to the next
-//             grid barrier
+//             and update their vertices (process_chunk).  Small colours (at
+//             most kPersistSmallBlocks blocks' worth of chunks, e.g. the
+//             107-vertex colours of a voxel cantilever) are done by the
+//             first S blocks only (S = blocks the largest small colour
+//             needs).  Colours are separated by neighbour-scoped readiness
+//             (PersistNbr, vbd_persist.h): a block waits only for the blocks
+//             that own vertices sharing a tet with its own vertices of the
+//             colour.  Without neighbour lists: a grid barrier between
+//             colours, and inside a run of small colours a barrier among the
+//             S blocks (__syncthreads when S = 1)
 //             end of sweep: block max of |dx_x+dx_y+dx_z| -> atomicMax on
 //             a rotating slot; the grid barrier; every block reads the slot
 //             and takes the same stop decision
@@ -90,6 +92,50 @@ __device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
   return v;
 }
 
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// This block has finished `phases` phases (sweep * ncolors + colour + 1):
+// every thread's writes of them are ordered before the release store.
+__device__ __forceinline__ void publish_epoch(const PersistNbr& nbr, unsigned long long phases) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release_u64(nbr.epoch + (size_t)blockIdx.x * kEpochStride, phases);
+  }
+}
+
+// Waits until every neighbour block listed for (this block, colour) has
+// published at least `need` phases.  The block's threads poll the list in
+// parallel, each wait bounded like the grid barrier's; returns false when a
+// wait expired here or elsewhere (the abort flag).
+__device__ __forceinline__ bool wait_neighbours(const PersistNbr& nbr, int list,
+                                                unsigned long long need, PersistCtl* ctl,
+                                                const PersistLimits& lim) {
+  const int b0 = __ldg(nbr.off + list), b1 = __ldg(nbr.off + list + 1);
+  int ok = 1;
+  for (int j = b0 + threadIdx.x; j < b1 && ok; j += blockDim.x) {
+    const unsigned long long* e = nbr.epoch + (size_t)__ldg(nbr.idx + j) * kEpochStride;
+    const unsigned long long t0 = globaltimer_ns();
+    for (long long n = 0;; ++n) {
+      if (ld_acquire_u64(e) >= need) break;
+      const bool expired = n >= lim.max_polls ||
+                           ((n & 255) == 255 && globaltimer_ns() - t0 > lim.max_wait_ns);
+      if (expired || ld_relaxed_u32(&ctl->abort) != 0u) {
+        if (expired) {
+          atomicOr(&ctl->status, kStatTimeout);
+          atomicExch(&ctl->abort, 1u);
+        }
+        ok = 0;
+        break;
+      }
+      __nanosleep(20);
+    }
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
 // Barrier on `counter` among the blocks that use it: passed when the counter
 // reaches `target` (the number of barriers so far x the participants).
 // Returns false if the launch is aborting (this block's wait expired, or
@@ -133,15 +179,12 @@ __device__ __forceinline__ bool grid_sync(PersistCtl* ctl, unsigned long long ta
   return counter_sync(ctl, &ctl->arrivals, target, lim, s_ok);
 }
 
-// A colour of at most kSmallBlocks x (warps per block) chunks is "small": it
-// runs on the first few blocks only.
-constexpr int kSmallBlocks = 8;
-
 template <typename Real, typename SReal, int TPV, int MAT, int FMT>
 __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
                                                       const StepParams* __restrict__ pp,
                                                       PersistCtl* ctl, PersistLimits lim,
-                                                      double* __restrict__ parts) {
+                                                      double* __restrict__ parts,
+                                                      PersistNbr nbr) {
   using S4 = real4<SReal>;
   __shared__ unsigned long long s_red[16];
   __shared__ double s_dsum[16];
@@ -271,7 +314,8 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
   }
   // small colours run on the first nsb blocks: as many as the largest of
   // them needs for one chunk per warp
-  auto is_small = [&](int nch) { return nb > 1 && nch <= kSmallBlocks * nwarps; };
+  auto is_small = [&](int nch) { return nb > 1 && nch <= kPersistSmallBlocks * nwarps; };
+  const bool scoped = nb > 1 && nbr.off != nullptr;
   int nsb = 1;
   for (int c = 0; c < e.ncolors; ++c) {
     const int nch = m.color[e.cbase + c].chunk_end - m.color[e.cbase + c].chunk_begin;
@@ -288,12 +332,23 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
       const ColorInfo ci = m.color[e.cbase + c];
       const bool small = is_small(ci.chunk_end - ci.chunk_begin);
       const int span = small ? nsb : nb;  // blocks that take this colour
+      const unsigned long long phase = (unsigned long long)it * e.ncolors + c;
+      // the first colour follows the end-of-sweep grid barrier
+      if (scoped && c > 0 &&
+          !wait_neighbours(nbr, blockIdx.x * e.ncolors + c, phase, ctl, lim)) {
+        if (threadIdx.x == 0) atomicOr(m.status, kStatTimeout);
+        return;
+      }
       if (blockIdx.x < span)
         for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
              q += span * nwarps)
           process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, cmax,
                                                     stat, tab, dxrec);
       if (c + 1 == e.ncolors) break;
+      if (scoped) {
+        publish_epoch(nbr, phase + 1);
+        continue;
+      }
       const ColorInfo cn = m.color[e.cbase + c + 1];
       if (small && is_small(cn.chunk_end - cn.chunk_begin)) {
         // both colours ran on the small-colour blocks only: they meet among
@@ -385,6 +440,7 @@ struct PersistLaunch {
   double* parts;
   size_t smem;
   cudaStream_t s;
+  PersistNbr nbr;
   template <typename Real, typename SReal, int TPV, int MAT, int FMT>
   cudaError_t run() {
     cudaError_t e = configure<Real, SReal, TPV, MAT, FMT>();
@@ -392,7 +448,7 @@ struct PersistLaunch {
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg = persist_config(blocks, threads, smem, s, attr);
     return cudaLaunchKernelEx(&cfg, persist_kernel<Real, SReal, TPV, MAT, FMT>, m, p, ctl, lim,
-                              parts);
+                              parts, nbr);
   }
 };
 
@@ -421,13 +477,15 @@ cudaError_t persist_occupancy(int prec, int material, int fmt, int tpv, int thre
 cudaError_t launch_persist(int prec, int material, int tpv, int threads, const DevMesh& m,
                            const StepParams* p, PersistCtl* ctl, int blocks,
                            const PersistLimits& lim, double* parts, size_t smem,
-                           cudaStream_t s) {
+                           const PersistNbr& nbr, cudaStream_t s) {
   if (threads < 32 || threads > 512 || threads % 32 || blocks < 1) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(PersistCtl), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(m.status, 0, sizeof(unsigned), s);
+  if (e == cudaSuccess && nbr.epoch)
+    e = cudaMemsetAsync(nbr.epoch, 0, sizeof(unsigned long long) * kEpochStride * blocks, s);
   if (e != cudaSuccess) return e;
   if (smem > (size_t)kPersistMaxTabSmem) return cudaErrorInvalidValue;
-  PersistLaunch f{blocks, threads, m, p, ctl, lim, parts, smem, s};
+  PersistLaunch f{blocks, threads, m, p, ctl, lim, parts, smem, s, nbr};
   return dispatch(prec, material, m.fmt, tpv, f);
 }
 

@@ -172,6 +172,9 @@ class VBDSolver:
                  type, then cached)
       coloring   per-vertex colours to use instead of the greedy colouring
       strict_spd raise instead of taking the guarded step on a non-SPD block
+      persist_sync  persistent mode: "neighbours" (default; each block waits
+                 between colours only for the blocks whose vertices share a
+                 tet with its own) or "grid" (a grid barrier between colours)
       allow_high_valence  lift the reference's 32 incident-tets limit
     """
 
@@ -180,7 +183,7 @@ class VBDSolver:
                  dx_tol=1e-9, max_iter=100, device="cuda", *, material="snh",
                  precision="fp64", mode="auto", tpv=0, block_threads=0, cluster=0, coloring=None,
                  strict_spd=False, allow_high_valence=False, verbose=False, order_index=False,
-                 tune=False):
+                 tune=False, persist_sync="neighbours"):
         L = _lib.load()
         if tune:
             from . import autotune
@@ -216,6 +219,10 @@ class VBDSolver:
             flags |= _lib.STRICT_SPD
         if order_index:
             flags |= _lib.ORDER_INDEX
+        if persist_sync not in ("neighbours", "grid"):
+            raise ValueError('persist_sync must be "neighbours" or "grid"')
+        if persist_sync == "grid":
+            flags |= _lib.PERSIST_GRID_BARRIERS
         flags |= _lib.cluster_flags(cluster)
         self.device = device
         self._dev = _device_index(device)
