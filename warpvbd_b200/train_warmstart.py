@@ -2,11 +2,12 @@
 
     python -m warpvbd_b200.train_warmstart [--out PATH] [--seed S] [--epochs E] [--lr LR]
 
-Generates 4.6M samples from seeded plain-VBD rollouts of 1000 steps, every
-25th step recorded (cantilever and mass-spring environments, E log-uniform
-in [1e5, 1e7] Pa, nu in [0.30, 0.48], random gravity direction per batch,
-N(0, 0.1^2) m/s initial velocity noise), trains the MLP for 24 epochs with the
-project's CUDA kernels and writes the model
+Generates about 11M samples from seeded plain-VBD rollouts of 1000 steps,
+every 25th step recorded (cantilever and mass-spring environments -- cubes of
+7-15 voxels under columns of 5-30, the range of the benchmark batch -- E
+log-uniform in [1e5, 1e7] Pa, nu in [0.30, 0.48], random gravity direction
+per batch, N(0, 0.1^2) m/s initial velocity noise), trains the MLP for 24
+epochs with the project's CUDA kernels and writes the model
 (parameters and normalisation) (default: warpvbd_b200/data/warmstart_mlp.npz).  Prints a JSON
 summary with the dataset size, the training loss curve, R^2 and timings.
 """
@@ -30,12 +31,20 @@ def main():
     ap.add_argument("--batch", type=int, default=4096, help="minibatch size")
     ap.add_argument("--fine", action="store_true",
                     help="include 1 m cantilevers of 40 and 80 voxels in the rollouts")
+    ap.add_argument("--target-tol", type=float, default=None,
+                    help="solve the recorded steps to this tolerance for their targets")
+    ap.add_argument("--cube", type=int, nargs=2, default=(7, 15),
+                    help="mass-spring cube edge range (voxels, inclusive)")
+    ap.add_argument("--column", type=int, nargs=2, default=(5, 30),
+                    help="mass-spring column length range (voxels, inclusive)")
     args = ap.parse_args()
     import torch
     t0 = time.perf_counter()
     X, Y = ws.rollout_dataset(seed=args.seed, n_batches=args.batches,
                               envs_per_batch=args.envs, steps=args.steps,
-                              record_every=args.every, fine=args.fine)
+                              record_every=args.every, fine=args.fine,
+                              target_tol=args.target_tol, cube=tuple(args.cube),
+                              column=tuple(args.column))
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     model, info = ws.train_warmstart(X, Y, epochs=args.epochs, batch=args.batch, lr=args.lr,

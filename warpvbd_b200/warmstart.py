@@ -146,12 +146,13 @@ class MLPTrainer:
         return self.P.detach().cpu().numpy().copy()
 
 
-def training_envs(seed, n_env, fine=False):
+def training_envs(seed, n_env, fine=False, cube=(5, 12), column=(3, 24)):
     """Seeded cantilever and mass-spring environments with random materials
     (E log-uniform in [1e5, 1e7] Pa, nu uniform in [0.30, 0.48]).  Cantilevers
     have 5 cm voxels (10-30 voxels long); with `fine`, every other one is a
     1 m beam of 40 or 80 voxels (2.5 / 1.25 cm) instead, so that beams of the
-    benchmark's resolutions are in the data too."""
+    benchmark's resolutions are in the data too.  Mass-springs: cube edge and
+    column length uniform integers in `cube` and `column` (inclusive)."""
     rng = np.random.default_rng(seed)
     envs = []
     for i in range(n_env):
@@ -165,25 +166,34 @@ def training_envs(seed, n_env, fine=False):
             envs.append(scenes.cantilever(n, max(1, n // 10), max(1, n // 10), length=n * 0.01 * 5,
                                           youngs=E, poisson=nu))
         else:
-            envs.append(scenes.mass_spring(int(rng.integers(5, 13)), int(rng.integers(3, 25)),
+            envs.append(scenes.mass_spring(int(rng.integers(cube[0], cube[1] + 1)),
+                                           int(rng.integers(column[0], column[1] + 1)),
                                            youngs=E, poisson=nu))
     return envs
 
 
 def rollout_dataset(seed=1, n_batches=6, envs_per_batch=24, steps=100, record_every=5,
                     dt=1e-3, tol=1e-7, max_iter=1000, velocity_noise=0.1, device="cuda",
-                    fine=False):
+                    fine=False, target_tol=None, target_max_iter=20000, cube=(5, 12),
+                    column=(3, 24)):
     """Plain-VBD rollouts on the GPU: every `record_every` steps the features
     at the step start and the correction the step converged to.  Each batch
     has its own random gravity direction; every active vertex starts with
     N(0, velocity_noise^2) velocity.  Returns (X [N, 24], Y [N, 3]) torch
-    tensors on the device."""
+    tensors on the device.
+
+    `target_tol`: the recorded steps are first solved to this tighter
+    tolerance (at most `target_max_iter` sweeps) for their targets -- the
+    step's converged solution rather than where VBD at `tol` stops -- and
+    then, from the same state, at `tol` to continue the rollout, so the
+    inputs follow the trajectories the solver runs at inference."""
     torch = _torch()
     from .batched import BatchedVBDSolver
     rng = np.random.default_rng(seed)
     Xs, Ys = [], []
     for b in range(n_batches):
-        envs = training_envs(int(rng.integers(1 << 31)), envs_per_batch, fine=fine)
+        envs = training_envs(int(rng.integers(1 << 31)), envs_per_batch, fine=fine, cube=cube,
+                             column=column)
         # batch 0 falls along -z; the others along a random direction
         d = np.array([0.0, 0.0, -1.0]) if b == 0 else rng.normal(size=3)
         g = 9.81 * d / np.linalg.norm(d)
@@ -201,8 +211,15 @@ def rollout_dataset(seed=1, n_batches=6, envs_per_batch=24, steps=100, record_ev
         for k in range(steps):
             if k % record_every == 0:
                 sol.ws_features(dt, feat)
-                sol.step(dt)
-                sol.ws_targets(feat, tgt)
+                if target_tol is not None:
+                    x0, v0 = sol.positions(), sol.velocities()
+                    sol.step(dt, dx_tol=target_tol, max_iter=target_max_iter)
+                    sol.ws_targets(feat, tgt)
+                    sol.set_state(positions=x0, velocities=v0)
+                    sol.step(dt)
+                else:
+                    sol.step(dt)
+                    sol.ws_targets(feat, tgt)
                 mask = feat[:, 23] > 0
                 Xs.append(feat[mask].clone())
                 Ys.append(tgt[mask].clone())
