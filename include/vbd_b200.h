@@ -61,6 +61,9 @@ typedef struct vbd_solver vbd_solver;
  * neighbour offsets: resolves position updates far below a 1e-7 m tolerance
  * at metre-scale displacements, which an fp32 state cannot */
 #define VBD_PRECISION_MIXED 0x20
+/* colour the mesh on the GPU at creation (vbd_graph_coloring_gpu; the same
+ * colours as the host pass) */
+#define VBD_GPU_SETUP 0x40
 #define VBD_MODE_AUTO 0x000
 #define VBD_MODE_BLOCK 0x100    /* one thread block per environment runs the whole step */
 #define VBD_MODE_GRAPH 0x200    /* per-colour kernels looped by a CUDA-graph conditional node */
@@ -101,6 +104,13 @@ int vbd_device_count(void);
  * count is written to *n_vertices_out and the colour count to *n_colors_out. */
 int vbd_graph_coloring(const int32_t* tets, int n_tets, int32_t* coloring_out,
                        int* n_vertices_out, int* n_colors_out);
+/* The same colouring computed on GPU `device` (coloring.py:40-72 replaced by
+ * Jones-Plassmann rounds with the vertex index as priority: a vertex takes
+ * the smallest colour its lower-indexed neighbours leave free once they all
+ * have one, which is exactly what the sequential pass gives it).  Host
+ * arrays in and out, as vbd_graph_coloring. */
+int vbd_graph_coloring_gpu(const int32_t* tets, int n_tets, int32_t* coloring_out,
+                           int* n_vertices_out, int* n_colors_out, int device);
 
 /* ---- solver ------------------------------------------------------------ */
 /* VBDSolver.__init__ (vbd_solver.py:367-498).

@@ -36,6 +36,7 @@ PRECISION_FP32 = 0x00
 PRECISION_FP64 = 0x10
 PRECISION_MIXED = 0x20
 PRECISIONS = {"fp32": PRECISION_FP32, "mixed": PRECISION_MIXED, "fp64": PRECISION_FP64}
+GPU_SETUP = 0x40
 MODE_AUTO = 0x000
 MODE_BLOCK = 0x100
 MODE_GRAPH = 0x200
@@ -86,6 +87,7 @@ SIGNATURES = {
     "vbd_last_error_message": (ctypes.c_char_p, []),
     "vbd_device_count": (ctypes.c_int, []),
     "vbd_graph_coloring": (ctypes.c_int, [_i, ctypes.c_int, _i, _ip, _ip]),
+    "vbd_graph_coloring_gpu": (ctypes.c_int, [_i, ctypes.c_int, _i, _ip, _ip, ctypes.c_int]),
     "vbd_create": (ctypes.c_int, [_d, ctypes.c_int, _i, ctypes.c_int, _d, _d, _d, _u8,
                                   ctypes.c_double, _d, _i, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),

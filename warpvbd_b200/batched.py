@@ -25,7 +25,7 @@ class BatchedVBDSolver:
     def __init__(self, envs, damping_coefficient=0.0, gravity=(0.0, 0.0, -9.81), dx_tol=1e-7,
                  max_iter=1000, device="cuda", *, material="snh", precision="fp64",
                  tpv=0, block_threads=0, cluster=0, order_index=False, tiered=False,
-                 tune=False):
+                 tune=False, gpu_setup=False):
         """``cluster``: blocks per thread-block cluster (0 = automatic); an
         environment much heavier than the others runs on a whole cluster.
         ``tiered``: run the environments split over a cluster in one launch
@@ -33,7 +33,8 @@ class BatchedVBDSolver:
         largest of them, in a second launch beside it.
         ``tune``: pick tpv / block_threads / cluster / order_index / tiered
         with the autotuner (warpvbd_b200.autotune; measured once, then
-        cached)."""
+        cached).  ``gpu_setup``: colour all environments in one GPU pass
+        (the same colours as the host's per-environment pass)."""
         if tune:
             from . import autotune
             cfg = autotune.tune_batched(envs, material=material, precision=precision,
@@ -73,6 +74,8 @@ class BatchedVBDSolver:
             flags |= _lib.ORDER_INDEX
         if tiered:
             flags |= _lib.TIERED
+        if gpu_setup:
+            flags |= _lib.GPU_SETUP
         L = _lib.load()
         h = ctypes.c_void_p()
         _lib.check(L.vbd_create_batched(

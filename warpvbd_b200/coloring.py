@@ -17,14 +17,22 @@ from . import _lib
 MAX_COLORS = 256  # coloring.py:50
 
 
-def color_tets(elements):
-    """Per-vertex colour (int32[max(elements)+1]) of the greedy colouring."""
+def color_tets(elements, device=None):
+    """Per-vertex colour (int32[max(elements)+1]) of the greedy colouring.
+    `device` (a CUDA device ordinal): compute it on that GPU with
+    vbd_graph_coloring_gpu -- Jones-Plassmann rounds with the vertex index as
+    priority, which give exactly the sequential pass's colours."""
     tets = _lib.i32(np.asarray(elements)).reshape(-1, 4)
     nv = int(tets.max()) + 1 if tets.size else 0
     out = np.empty(max(nv, 1), dtype=np.int32)
     n_v, n_c = ctypes.c_int(0), ctypes.c_int(0)
-    st = _lib.load().vbd_graph_coloring(_lib.ptr(tets, "i"), tets.shape[0], _lib.ptr(out, "i"),
-                                        ctypes.byref(n_v), ctypes.byref(n_c))
+    L = _lib.load()
+    if device is None:
+        st = L.vbd_graph_coloring(_lib.ptr(tets, "i"), tets.shape[0], _lib.ptr(out, "i"),
+                                  ctypes.byref(n_v), ctypes.byref(n_c))
+    else:
+        st = L.vbd_graph_coloring_gpu(_lib.ptr(tets, "i"), tets.shape[0], _lib.ptr(out, "i"),
+                                      ctypes.byref(n_v), ctypes.byref(n_c), int(device))
     if st == _lib.ERR_TOO_MANY_COLORS:
         raise AssertionError("Exceeded maximum number of colors")
     _lib.check(st, "vbd_graph_coloring")

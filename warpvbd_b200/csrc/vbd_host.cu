@@ -25,6 +25,7 @@
 #include "vbd_launch.h"
 #include "vbd_persist.h"
 #include "vbd_noalloc.h"
+#include "vbd_setup.h"
 #include "vbd_warmstart.h"
 
 using namespace vbd;
@@ -219,10 +220,14 @@ struct Layout {
   long long n_slots = 0;
 };
 
+// `greedy`: the greedy colouring of the whole mesh, already computed (on the
+// GPU); every environment's colours are its slice (environments share no tet,
+// so a vertex's lower neighbours all lie in its environment).  Null: the
+// colouring is computed here per environment.
 int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8_t* active,
                  const std::vector<int>& voff, const std::vector<int>& toff,
                  const int32_t* coloring, const TetData& td, int tpv, bool order_index,
-                 Layout& L) {
+                 Layout& L, const int32_t* greedy = nullptr) {
   const int n_env = (int)voff.size() - 1;
   const int cpw = 32 / tpv;
   L.new_of_old.assign(V, -1);
@@ -261,6 +266,12 @@ int build_layout(const double* X, int V, const int32_t* tets, int T, const uint8
               return fail(VBD_ERR_INVALID_ARG,
                           "coloring gives two vertices of tet " + std::to_string(t) +
                               " the same colour");
+    } else if (tn > 0 && greedy) {
+      // as the per-environment pass colours them: ids 0 .. max local id
+      for (int v = 0; v < nv_col; ++v) {
+        col[v] = greedy[vo + v];
+        ncol = std::max(ncol, col[v] + 1);
+      }
     } else if (tn > 0) {
       ncol = greedy_coloring(lt.data(), tn, nv_col, col.data());
       if (ncol < 0) return fail(VBD_ERR_TOO_MANY_COLORS, "Exceeded maximum number of colors");
@@ -938,6 +949,22 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
     delete s;
     return rc;
   }
+  // VBD_GPU_SETUP: the greedy colouring of the whole mesh on the GPU (the
+  // same colours as the per-environment host pass)
+  std::vector<int32_t> gpu_colors;
+  if ((flags & VBD_GPU_SETUP) && !coloring && T > 0) {
+    gpu_colors.assign(V, -1);
+    std::string why;
+    const int nc = gpu_greedy_coloring(tets, T, V, gpu_colors.data(), nullptr, &why);
+    if (nc == kSetupTooManyColors) {
+      delete s;
+      return fail(VBD_ERR_TOO_MANY_COLORS, "Exceeded maximum number of colors");
+    }
+    if (nc < 0) {
+      delete s;
+      return fail(VBD_ERR_CUDA, "GPU colouring: " + why);
+    }
+  }
   // mode / threads / tpv
   int mode = flags & VBD_MODE_MASK;
   // provisional environment size bound for the shared-memory check
@@ -996,9 +1023,11 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
       std::vector<int32_t> col(V, -1);
       int nvc = 0;
       for (size_t i = 0; i < 4 * (size_t)T; ++i) nvc = std::max(nvc, tets[i] + 1);
-      int ncol = coloring ? 0 : greedy_coloring(tets, T, nvc, col.data());
-      if (coloring) {
-        for (int v = 0; v < nvc; ++v) col[v] = coloring[v];
+      const int32_t* pre =
+          coloring ? coloring : (gpu_colors.empty() ? nullptr : gpu_colors.data());
+      int ncol = pre ? 0 : greedy_coloring(tets, T, nvc, col.data());
+      if (pre) {
+        for (int v = 0; v < nvc; ++v) col[v] = pre[v];
         for (int v = 0; v < nvc; ++v) ncol = std::max(ncol, col[v] + 1);
       }
       std::vector<int> cnt(std::max(ncol, 1), 0);
@@ -1014,7 +1043,8 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   s->tpv = tpv;
   s->L.table.fp64 = s->fp64;
   rc = build_layout(X, V, tets, T, active, voff, toff, coloring, td, tpv,
-                    (flags & VBD_ORDER_INDEX) != 0, s->L);
+                    (flags & VBD_ORDER_INDEX) != 0, s->L,
+                    gpu_colors.empty() ? nullptr : gpu_colors.data());
   if (rc != VBD_OK) {
     delete s;
     return rc;
@@ -1563,6 +1593,30 @@ int vbd_graph_coloring(const int32_t* tets, int n_tets, int32_t* coloring_out,
   int nc = nv ? greedy_coloring(tets, n_tets, nv, coloring_out) : 0;
   if (n_vertices_out) *n_vertices_out = nv;
   if (nc < 0) return fail(VBD_ERR_TOO_MANY_COLORS, "Exceeded maximum number of colors");
+  if (n_colors_out) *n_colors_out = nc;
+  return VBD_OK;
+}
+
+int vbd_graph_coloring_gpu(const int32_t* tets, int n_tets, int32_t* coloring_out,
+                           int* n_vertices_out, int* n_colors_out, int device) {
+  if (n_tets < 0 || (n_tets > 0 && (!tets || !coloring_out)))
+    return fail(VBD_ERR_INVALID_ARG, "bad arguments");
+  int nv = 0;
+  for (size_t i = 0; i < 4 * (size_t)n_tets; ++i) {
+    if (tets[i] < 0) return fail(VBD_ERR_INVALID_ARG, "negative vertex id");
+    nv = std::max(nv, tets[i] + 1);
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(VBD_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(VBD_ERR_INVALID_ARG, "bad device ordinal");
+  DeviceGuard dg(device);
+  std::string why;
+  const int nc = nv ? gpu_greedy_coloring(tets, n_tets, nv, coloring_out, nullptr, &why) : 0;
+  if (n_vertices_out) *n_vertices_out = nv;
+  if (nc == kSetupTooManyColors)
+    return fail(VBD_ERR_TOO_MANY_COLORS, "Exceeded maximum number of colors");
+  if (nc < 0) return fail(VBD_ERR_CUDA, "GPU colouring: " + why);
   if (n_colors_out) *n_colors_out = nc;
   return VBD_OK;
 }

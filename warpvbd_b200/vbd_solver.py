@@ -172,6 +172,8 @@ class VBDSolver:
                  type, then cached)
       coloring   per-vertex colours to use instead of the greedy colouring
       strict_spd raise instead of taking the guarded step on a non-SPD block
+      gpu_setup  colour the mesh on the GPU at construction (the same colours as
+                 the host pass; vbd_graph_coloring_gpu)
       persist_sync  persistent mode: "neighbours" (default; each block waits
                  between colours only for the blocks whose vertices share a
                  tet with its own) or "grid" (a grid barrier between colours)
@@ -183,7 +185,7 @@ class VBDSolver:
                  dx_tol=1e-9, max_iter=100, device="cuda", *, material="snh",
                  precision="fp64", mode="auto", tpv=0, block_threads=0, cluster=0, coloring=None,
                  strict_spd=False, allow_high_valence=False, verbose=False, order_index=False,
-                 tune=False, persist_sync="neighbours"):
+                 tune=False, persist_sync="neighbours", gpu_setup=False):
         L = _lib.load()
         if tune:
             from . import autotune
@@ -223,6 +225,8 @@ class VBDSolver:
             raise ValueError('persist_sync must be "neighbours" or "grid"')
         if persist_sync == "grid":
             flags |= _lib.PERSIST_GRID_BARRIERS
+        if gpu_setup:
+            flags |= _lib.GPU_SETUP
         flags |= _lib.cluster_flags(cluster)
         self.device = device
         self._dev = _device_index(device)
