@@ -28,6 +28,7 @@
 #ifndef VBD_B200_H
 #define VBD_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -281,11 +282,16 @@ int vbd_get_env_status(vbd_solver* s, uint32_t* status_out);
  * first batch rows) of X [N][feature_width] and Y [N][3]; writes the loss
  * gradient with respect to params into grad and adds sum of squared errors to
  * *loss (device double, may be NULL).  scratch: device floats, at least
- * batch * (4 * 64 + 3).  Enqueued on `stream`. */
+ * vbd_mlp_train_scratch_floats(batch) of them (one partial gradient per
+ * 32-sample tile; the tiles' partials are added in tile order, so the
+ * gradient is the same on every run).  Enqueued on `stream`. */
 int vbd_mlp_train_batch(const float* X, const float* Y, const int32_t* idx, int batch,
                         const float* params, float* grad, float* scratch, double* loss,
                         void* stream);
-/* fp32 forward pass: out [n][3] (device); scratch: at least n * 128 floats. */
+/* Scratch floats vbd_mlp_train_batch needs for a minibatch of `batch` rows:
+ * ceil(batch / 32) * (parameter count + 1). */
+size_t vbd_mlp_train_scratch_floats(int batch);
+/* fp32 forward pass: out [n][3] (device); scratch: not used, may be NULL. */
 int vbd_mlp_forward(const float* X, int n, const float* params, float* out, float* scratch,
                     void* stream);
 /* Adam update of n parameters, step t >= 1 (device arrays). */

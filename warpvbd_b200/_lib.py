@@ -131,6 +131,7 @@ SIGNATURES = {
     "vbd_mlp_train_batch": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp,
                                            _vp]),
     "vbd_mlp_forward": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "vbd_mlp_train_scratch_floats": (ctypes.c_size_t, [ctypes.c_int]),
     "vbd_mlp_adam": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                     _vp]),

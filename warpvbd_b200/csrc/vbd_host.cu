@@ -1995,11 +1995,16 @@ int vbd_mlp_train_batch(const float* X, const float* Y, const int32_t* idx, int 
   return VBD_OK;
 }
 
+size_t vbd_mlp_train_scratch_floats(int batch) {
+  return batch > 0 ? mlp_train_scratch_floats(batch) : 0;
+}
+
 int vbd_mlp_forward(const float* X, int n, const float* params, float* out, float* scratch,
                     void* stream) {
-  if (!X || !params || !out || !scratch || n < 0) return fail(VBD_ERR_INVALID_ARG, "bad arguments");
+  (void)scratch;
+  if (!X || !params || !out || n < 0) return fail(VBD_ERR_INVALID_ARG, "bad arguments");
   if (n == 0) return VBD_OK;
-  CUDA_TRY(launch_mlp_forward(X, n, params, out, scratch, static_cast<cudaStream_t>(stream)));
+  CUDA_TRY(launch_mlp_forward(X, n, params, out, static_cast<cudaStream_t>(stream)));
   return VBD_OK;
 }
 

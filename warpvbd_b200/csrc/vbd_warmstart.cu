@@ -190,119 +190,207 @@ __global__ void ws_targets_kernel(DevMesh m, const float* __restrict__ feat,
 }
 
 // ---------------------------------------------------------------------------
-// Training (fp32).  A minibatch is a list of row indices into X [N][24] and
-// Y [N][3].  Per sample: forward keeping the pre-activations A1, A2; the loss
-// gradient dOut = 2 (out - y) / (3 B); backward to the pre-activation
-// gradients D1, D2.  Weight gradients reduce over the minibatch with one
-// thread per parameter.
+// Forward pass (fp32, one thread per sample), for evaluation: X [n][24] ->
+// out [n][3].
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) mlp_forward_kernel(
-    const float* __restrict__ X, const float* __restrict__ Y, const int* __restrict__ idx,
-    int batch, const float* __restrict__ P, float* __restrict__ A1, float* __restrict__ A2,
-    float* __restrict__ dout, double* __restrict__ loss, float* __restrict__ out_pred) {
+__global__ void __launch_bounds__(128) mlp_forward_kernel(const float* __restrict__ X, int n,
+                                                          const float* __restrict__ P,
+                                                          float* __restrict__ out) {
   __shared__ float W[kWsParams];
   for (int i = threadIdx.x; i < kWsParams; i += blockDim.x) W[i] = P[i];
   __syncthreads();
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  double l = 0.0;
-  if (b < batch) {
-    const int r = idx ? idx[b] : b;
-    const float* x = X + (size_t)r * kWsRow;
-    float h1[kWsHidden];
-#pragma unroll
-    for (int j = 0; j < kWsHidden; ++j) {
-      float a = W[kWsB1 + j];
-#pragma unroll
-      for (int i = 0; i < kWsIn; ++i) a += W[kWsW1 + j * kWsIn + i] * x[i];
-      A1[(size_t)b * kWsHidden + j] = a;
-      h1[j] = silu(a);
-    }
-    float o[kWsOut] = {W[kWsB3], W[kWsB3 + 1], W[kWsB3 + 2]};
-    for (int j = 0; j < kWsHidden; ++j) {
-      float a = W[kWsB2 + j];
-#pragma unroll
-      for (int i = 0; i < kWsHidden; ++i) a += W[kWsW2 + j * kWsHidden + i] * h1[i];
-      A2[(size_t)b * kWsHidden + j] = a;
-      const float s = silu(a);
-      for (int k = 0; k < kWsOut; ++k) o[k] += W[kWsW3 + k * kWsHidden + j] * s;
-    }
-    for (int k = 0; k < kWsOut; ++k) {
-      if (out_pred) out_pred[(size_t)b * kWsOut + k] = o[k];
-      if (Y) {
-        const float d = o[k] - Y[(size_t)r * kWsOut + k];
-        dout[(size_t)b * kWsOut + k] = 2.0f * d / (kWsOut * batch);
-        l += double(d) * d;
-      }
-    }
-  }
-  if (loss) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) l += __shfl_xor_sync(0xffffffffu, l, off);
-    if ((threadIdx.x & 31) == 0 && l != 0.0) atomicAdd(loss, l);
-  }
-}
-
-__global__ void __launch_bounds__(128) mlp_backward_kernel(int batch, const float* __restrict__ P,
-                                                           const float* __restrict__ A1,
-                                                           const float* __restrict__ A2,
-                                                           const float* __restrict__ dout,
-                                                           float* __restrict__ D1,
-                                                           float* __restrict__ D2) {
-  __shared__ float W[kWsParams];
-  for (int i = threadIdx.x; i < kWsParams; i += blockDim.x) W[i] = P[i];
-  __syncthreads();
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= batch) return;
-  float d2[kWsHidden];
-  const float g0 = dout[(size_t)b * kWsOut], g1 = dout[(size_t)b * kWsOut + 1],
-              g2 = dout[(size_t)b * kWsOut + 2];
+  if (b >= n) return;
+  const float* x = X + (size_t)b * kWsRow;
+  float h1[kWsHidden];
 #pragma unroll
   for (int j = 0; j < kWsHidden; ++j) {
-    const float gh = W[kWsW3 + j] * g0 + W[kWsW3 + kWsHidden + j] * g1 +
-                     W[kWsW3 + 2 * kWsHidden + j] * g2;
-    d2[j] = gh * silu_grad(A2[(size_t)b * kWsHidden + j]);
-    D2[(size_t)b * kWsHidden + j] = d2[j];
+    float a = W[kWsB1 + j];
+#pragma unroll
+    for (int i = 0; i < kWsIn; ++i) a += W[kWsW1 + j * kWsIn + i] * x[i];
+    h1[j] = silu(a);
   }
-  for (int i = 0; i < kWsHidden; ++i) {
+  float o[kWsOut] = {W[kWsB3], W[kWsB3 + 1], W[kWsB3 + 2]};
+  for (int j = 0; j < kWsHidden; ++j) {
+    float a = W[kWsB2 + j];
+#pragma unroll
+    for (int i = 0; i < kWsHidden; ++i) a += W[kWsW2 + j * kWsHidden + i] * h1[i];
+    const float s = silu(a);
+    for (int k = 0; k < kWsOut; ++k) o[k] += W[kWsW3 + k * kWsHidden + j] * s;
+  }
+  for (int k = 0; k < kWsOut; ++k) out[(size_t)b * kWsOut + k] = o[k];
+}
+
+// ---------------------------------------------------------------------------
+// Training step, fused per tile of kTrainTile samples (one block): forward
+// with the activations kept in shared memory, the loss gradient, backward to
+// the pre-activation deltas, and the tile's partial weight gradients -- each
+// parameter's sum over the tile's samples.  A second kernel adds the tiles'
+// partials in tile order, so the gradient is the same on every run (no
+// atomics).  Mapping: thread t handles column (hidden unit) t % 64 for the
+// samples t / 64, t / 64 + 4, ...; weights are staged in shared memory, W1
+// and W2 transposed for the forward pass so that consecutive threads read
+// consecutive words.
+// ---------------------------------------------------------------------------
+constexpr int kTrainTile = 32;
+constexpr int kTrainThreads = 256;
+constexpr int kTrainPartial = kWsParams + 1;  // + the tile's sum of squared errors
+// shared-memory map (floats)
+constexpr int kTsW = 0;                                   // params as stored
+constexpr int kTsW1T = kTsW + kWsParams;                  // W1^T [22][64]
+constexpr int kTsW2T = kTsW1T + kWsIn * kWsHidden;        // W2^T [64][64]
+constexpr int kTsX = kTsW2T + kWsHidden * kWsHidden;      // X [tile][22]
+constexpr int kTsS1 = kTsX + kTrainTile * kWsIn;          // silu(A1) [tile][64]
+constexpr int kTsG1 = kTsS1 + kTrainTile * kWsHidden;     // silu'(A1)
+constexpr int kTsS2 = kTsG1 + kTrainTile * kWsHidden;     // silu(A2)
+constexpr int kTsG2 = kTsS2 + kTrainTile * kWsHidden;     // silu'(A2)
+constexpr int kTsD1 = kTsG2 + kTrainTile * kWsHidden;     // dL/dA1
+constexpr int kTsD2 = kTsD1 + kTrainTile * kWsHidden;     // dL/dA2
+constexpr int kTsOut = kTsD2 + kTrainTile * kWsHidden;    // dL/dout [tile][3]
+constexpr int kTsSse = kTsOut + kTrainTile * kWsOut;      // per-warp squared errors
+constexpr int kTsFloats = kTsSse + kTrainThreads / 32;
+constexpr size_t kTrainSmem = sizeof(float) * kTsFloats;
+
+__global__ void __launch_bounds__(kTrainThreads) mlp_train_tile_kernel(
+    const float* __restrict__ X, const float* __restrict__ Y, const int* __restrict__ idx,
+    int batch, const float* __restrict__ P, float* __restrict__ out) {
+  extern __shared__ __align__(16) float ts[];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int s0 = blockIdx.x * kTrainTile;
+  const int ns = min(kTrainTile, batch - s0);
+  for (int i = t; i < kWsParams; i += kTrainThreads) ts[kTsW + i] = P[i];
+  for (int i = t; i < kWsHidden * kWsIn; i += kTrainThreads) {
+    const int j = i / kWsIn, k = i % kWsIn;
+    ts[kTsW1T + k * kWsHidden + j] = P[kWsW1 + i];
+  }
+  for (int i = t; i < kWsHidden * kWsHidden; i += kTrainThreads) {
+    const int j = i / kWsHidden, k = i % kWsHidden;
+    ts[kTsW2T + k * kWsHidden + j] = P[kWsW2 + i];
+  }
+  for (int i = t; i < kTrainTile * kWsIn; i += kTrainThreads) {
+    const int s = i / kWsIn, k = i % kWsIn;
+    float v = 0.0f;
+    if (s < ns) {
+      const int r = idx ? idx[s0 + s] : s0 + s;
+      v = X[(size_t)r * kWsRow + k];
+    }
+    ts[kTsX + i] = v;
+  }
+  __syncthreads();
+  const int j = t & (kWsHidden - 1), sg = t / kWsHidden, sstride = kTrainThreads / kWsHidden;
+  // layer 1
+  for (int s = sg; s < kTrainTile; s += sstride) {
+    float a = ts[kTsW + kWsB1 + j];
+#pragma unroll
+    for (int k = 0; k < kWsIn; ++k) a += ts[kTsW1T + k * kWsHidden + j] * ts[kTsX + s * kWsIn + k];
+    ts[kTsS1 + s * kWsHidden + j] = silu(a);
+    ts[kTsG1 + s * kWsHidden + j] = silu_grad(a);
+  }
+  __syncthreads();
+  // layer 2
+  for (int s = sg; s < kTrainTile; s += sstride) {
+    float a = ts[kTsW + kWsB2 + j];
+#pragma unroll 16
+    for (int k = 0; k < kWsHidden; ++k)
+      a += ts[kTsW2T + k * kWsHidden + j] * ts[kTsS1 + s * kWsHidden + k];
+    ts[kTsS2 + s * kWsHidden + j] = silu(a);
+    ts[kTsG2 + s * kWsHidden + j] = silu_grad(a);
+  }
+  __syncthreads();
+  // layer 3 and the loss gradient: one warp per (sample, output), two hidden
+  // units per lane and a shuffle reduction
+  float sse = 0.0f;
+  for (int o = warp; o < kTrainTile * kWsOut; o += kTrainThreads / 32) {
+    const int s = o / kWsOut, k = o % kWsOut;
+    float a = ts[kTsW + kWsW3 + k * kWsHidden + lane] * ts[kTsS2 + s * kWsHidden + lane] +
+              ts[kTsW + kWsW3 + k * kWsHidden + lane + 32] * ts[kTsS2 + s * kWsHidden + lane + 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    if (lane == 0) {
+      float g = 0.0f;
+      if (s < ns) {
+        const int r = idx ? idx[s0 + s] : s0 + s;
+        const float d = a + ts[kTsW + kWsB3 + k] - Y[(size_t)r * kWsOut + k];
+        g = 2.0f * d / (kWsOut * batch);
+        sse += d * d;
+      }
+      ts[kTsOut + o] = g;
+    }
+  }
+  if (lane == 0) ts[kTsSse + warp] = sse;
+  __syncthreads();
+  // backward: layer-2 deltas, then layer-1 deltas
+  for (int s = sg; s < kTrainTile; s += sstride) {
     float gh = 0.0f;
 #pragma unroll
-    for (int j = 0; j < kWsHidden; ++j) gh += W[kWsW2 + j * kWsHidden + i] * d2[j];
-    D1[(size_t)b * kWsHidden + i] = gh * silu_grad(A1[(size_t)b * kWsHidden + i]);
+    for (int k = 0; k < kWsOut; ++k)
+      gh += ts[kTsW + kWsW3 + k * kWsHidden + j] * ts[kTsOut + s * kWsOut + k];
+    ts[kTsD2 + s * kWsHidden + j] = gh * ts[kTsG2 + s * kWsHidden + j];
+  }
+  __syncthreads();
+  for (int s = sg; s < kTrainTile; s += sstride) {
+    float gh = 0.0f;
+#pragma unroll 16
+    for (int k = 0; k < kWsHidden; ++k)
+      gh += ts[kTsW + kWsW2 + k * kWsHidden + j] * ts[kTsD2 + s * kWsHidden + k];
+    ts[kTsD1 + s * kWsHidden + j] = gh * ts[kTsG1 + s * kWsHidden + j];
+  }
+  __syncthreads();
+  // the tile's weight gradients: each parameter summed over the tile's
+  // samples (padding samples have zero deltas)
+  float* dst = out + (size_t)blockIdx.x * kTrainPartial;
+  for (int p = t; p < kWsParams; p += kTrainThreads) {
+    const float *a, *b;
+    int sa, sb;
+    if (p < kWsB1) {  // W1[j][i] += D1[s][j] X[s][i]
+      a = ts + kTsD1 + p / kWsIn; sa = kWsHidden;
+      b = ts + kTsX + p % kWsIn; sb = kWsIn;
+    } else if (p < kWsW2) {  // b1[j]
+      a = ts + kTsD1 + (p - kWsB1); sa = kWsHidden; b = nullptr; sb = 0;
+    } else if (p < kWsB2) {  // W2[j][i] += D2[s][j] S1[s][i]
+      a = ts + kTsD2 + (p - kWsW2) / kWsHidden; sa = kWsHidden;
+      b = ts + kTsS1 + (p - kWsW2) % kWsHidden; sb = kWsHidden;
+    } else if (p < kWsW3) {  // b2[j]
+      a = ts + kTsD2 + (p - kWsB2); sa = kWsHidden; b = nullptr; sb = 0;
+    } else if (p < kWsB3) {  // W3[k][j] += dout[s][k] S2[s][j]
+      a = ts + kTsOut + (p - kWsW3) / kWsHidden; sa = kWsOut;
+      b = ts + kTsS2 + (p - kWsW3) % kWsHidden; sb = kWsHidden;
+    } else {  // b3[k]
+      a = ts + kTsOut + (p - kWsB3); sa = kWsOut; b = nullptr; sb = 0;
+    }
+    float acc = 0.0f;
+    if (b) {
+#pragma unroll 8
+      for (int s = 0; s < kTrainTile; ++s) acc += a[s * sa] * b[s * sb];
+    } else {
+#pragma unroll 8
+      for (int s = 0; s < kTrainTile; ++s) acc += a[s * sa];
+    }
+    dst[p] = acc;
+  }
+  if (t == 0) {
+    float v = 0.0f;
+    for (int w = 0; w < kTrainThreads / 32; ++w) v += ts[kTsSse + w];
+    dst[kWsParams] = v;
   }
 }
 
-// One thread per parameter: sum over the minibatch of its gradient terms.
-__global__ void __launch_bounds__(256) mlp_wgrad_kernel(
-    const float* __restrict__ X, const int* __restrict__ idx, int batch,
-    const float* __restrict__ A1, const float* __restrict__ A2, const float* __restrict__ D1,
-    const float* __restrict__ D2, const float* __restrict__ dout, float* __restrict__ grad) {
+// Sum of the tiles' partial gradients in tile order (and of their squared
+// errors into *loss).
+__global__ void mlp_reduce_tiles_kernel(const float* __restrict__ part, int tiles,
+                                        float* __restrict__ grad, double* __restrict__ loss) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= kWsParams) return;
-  float acc = 0.0f;
-  if (p < kWsB1) {  // W1[j][i]
-    const int j = p / kWsIn, i = p % kWsIn;
-    for (int b = 0; b < batch; ++b) {
-      const int r = idx ? idx[b] : b;
-      acc += D1[(size_t)b * kWsHidden + j] * X[(size_t)r * kWsRow + i];
+  if (p > kWsParams) return;
+  if (p == kWsParams) {
+    if (loss) {
+      double v = 0.0;
+      for (int b = 0; b < tiles; ++b) v += double(part[(size_t)b * kTrainPartial + p]);
+      *loss += v;
     }
-  } else if (p < kWsW2) {  // b1[j]
-    const int j = p - kWsB1;
-    for (int b = 0; b < batch; ++b) acc += D1[(size_t)b * kWsHidden + j];
-  } else if (p < kWsB2) {  // W2[j][i]
-    const int j = (p - kWsW2) / kWsHidden, i = (p - kWsW2) % kWsHidden;
-    for (int b = 0; b < batch; ++b)
-      acc += D2[(size_t)b * kWsHidden + j] * silu(A1[(size_t)b * kWsHidden + i]);
-  } else if (p < kWsW3) {  // b2[j]
-    const int j = p - kWsB2;
-    for (int b = 0; b < batch; ++b) acc += D2[(size_t)b * kWsHidden + j];
-  } else if (p < kWsB3) {  // W3[k][j]
-    const int k = (p - kWsW3) / kWsHidden, j = (p - kWsW3) % kWsHidden;
-    for (int b = 0; b < batch; ++b)
-      acc += dout[(size_t)b * kWsOut + k] * silu(A2[(size_t)b * kWsHidden + j]);
-  } else {  // b3[k]
-    const int k = p - kWsB3;
-    for (int b = 0; b < batch; ++b) acc += dout[(size_t)b * kWsOut + k];
+    return;
   }
+  float acc = 0.0f;
+  for (int b = 0; b < tiles; ++b) acc += part[(size_t)b * kTrainPartial + p];
   grad[p] = acc;
 }
 
@@ -377,28 +465,29 @@ cudaError_t launch_to_bf16(const float* P, void* out, int n, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+size_t mlp_train_scratch_floats(int batch) {
+  return (size_t)nblk(batch, kTrainTile) * kTrainPartial;
+}
+
 cudaError_t launch_mlp_train_batch(const float* X, const float* Y, const int* idx, int batch,
                                    const float* P, float* grad, float* scratch, double* loss,
                                    cudaStream_t s) {
-  float* A1 = scratch;
-  float* A2 = A1 + (size_t)batch * kWsHidden;
-  float* D1 = A2 + (size_t)batch * kWsHidden;
-  float* D2 = D1 + (size_t)batch * kWsHidden;
-  float* dout = D2 + (size_t)batch * kWsHidden;
-  mlp_forward_kernel<<<nblk(batch, 128), 128, 0, s>>>(X, Y, idx, batch, P, A1, A2, dout, loss,
-                                                      nullptr);
-  mlp_backward_kernel<<<nblk(batch, 128), 128, 0, s>>>(batch, P, A1, A2, dout, D1, D2);
-  mlp_wgrad_kernel<<<nblk(kWsParams, 256), 256, 0, s>>>(X, idx, batch, A1, A2, D1, D2, dout,
-                                                        grad);
+  static bool attr_set = false;  // per process; the attribute is per function
+  if (!attr_set) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        mlp_train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  const int tiles = nblk(batch, kTrainTile);
+  mlp_train_tile_kernel<<<tiles, kTrainThreads, kTrainSmem, s>>>(X, Y, idx, batch, P, scratch);
+  mlp_reduce_tiles_kernel<<<nblk(kTrainPartial, 256), 256, 0, s>>>(scratch, tiles, grad, loss);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_forward(const float* X, int n, const float* P, float* out,
-                               float* scratch, cudaStream_t s) {
-  float* A1 = scratch;
-  float* A2 = A1 + (size_t)n * kWsHidden;
-  mlp_forward_kernel<<<nblk(n, 128), 128, 0, s>>>(X, nullptr, nullptr, n, P, A1, A2, nullptr,
-                                                  nullptr, out);
+                               cudaStream_t s) {
+  if (n > 0) mlp_forward_kernel<<<nblk(n, 128), 128, 0, s>>>(X, n, P, out);
   return cudaGetLastError();
 }
 

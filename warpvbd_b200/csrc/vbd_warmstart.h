@@ -21,8 +21,6 @@ constexpr int kWsB3 = kWsW3 + kWsOut * kWsHidden;
 constexpr int kWsParams = kWsB3 + kWsOut;  // 5827
 // normalisation: mean[22], 1/std[22] of the inputs, std[3], mean[3] of the targets
 constexpr int kWsNorm = 2 * kWsIn + 2 * kWsOut;  // 50
-// floats of training scratch per minibatch sample: A1, A2, D1, D2, dOut
-constexpr int kWsScratchPerSample = 4 * kWsHidden + kWsOut;
 
 // `pack`: scratch of 6 floats per vertex (the packed fp32 displacement and
 // velocity the neighbour sums read, rewritten by every call).
@@ -38,8 +36,10 @@ cudaError_t launch_to_bf16(const float* P, void* out, int n, cudaStream_t s);
 cudaError_t launch_mlp_train_batch(const float* X, const float* Y, const int* idx, int batch,
                                    const float* P, float* grad, float* scratch, double* loss,
                                    cudaStream_t s);
-cudaError_t launch_mlp_forward(const float* X, int n, const float* P, float* out,
-                               float* scratch, cudaStream_t s);
+// floats of training scratch for a minibatch: one partial gradient (and sum
+// of squared errors) per 32-sample tile
+size_t mlp_train_scratch_floats(int batch);
+cudaError_t launch_mlp_forward(const float* X, int n, const float* P, float* out, cudaStream_t s);
 cudaError_t launch_adam(float* P, const float* G, float* M, float* V, int n, float lr,
                         float beta1, float beta2, float eps, int t, cudaStream_t s);
 

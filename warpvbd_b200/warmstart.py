@@ -85,7 +85,8 @@ class MLPTrainer:
         self.M = torch.zeros_like(self.P)
         self.V = torch.zeros_like(self.P)
         self.max_batch = max_batch
-        self.scratch = torch.empty(max_batch * (4 * N_HID + N_OUT), device=self.device)
+        self.scratch = torch.empty(_lib.load().vbd_mlp_train_scratch_floats(max_batch),
+                                   device=self.device)
         self.loss = torch.zeros(1, dtype=torch.float64, device=self.device)
         self.t = 0
         self.stream = torch.cuda.current_stream(self.device).cuda_stream
@@ -113,9 +114,8 @@ class MLPTrainer:
         torch = self.torch
         n = X.shape[0]
         out = torch.empty((n, N_OUT), device=self.device)
-        scratch = torch.empty(max(n, 1) * 2 * N_HID, device=self.device)
         _lib.check(_lib.load().vbd_mlp_forward(_ptr(X), n, _ptr(self.P), _ptr(out),
-                                               _ptr(scratch), ctypes.c_void_p(self.stream)),
+                                               None, ctypes.c_void_p(self.stream)),
                    "vbd_mlp_forward")
         return out
 
