@@ -2,7 +2,7 @@
 
     python -m warpvbd_b200.train_warmstart [--out PATH] [--seed S] [--epochs E] [--lr LR]
 
-Generates about 11M samples from seeded plain-VBD rollouts of 1000 steps,
+Generates about 8.2M samples from seeded plain-VBD rollouts of 1000 steps,
 every 25th step recorded (cantilever and mass-spring environments -- cubes of
 7-15 voxels under columns of 5-30, the range of the benchmark batch -- E
 log-uniform in [1e5, 1e7] Pa, nu in [0.30, 0.48], random gravity direction
