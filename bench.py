@@ -24,7 +24,9 @@ timed window does not start from rest: every timed run first advances its
 solver ``--start-step`` steps (default 500, the middle of the trajectory)
 untimed, then takes the warm-up and timed steps.  ``batch_1000_steps``
 reports the whole trajectory from rest, plain and warm-started, every step
-device-timed.
+device-timed, with each environment's tip displacement every 100 steps: the
+warm-started run's against plain VBD's at the same tolerance, and both
+against a plain run at tol 1e-9 (the accuracy each form buys at tol 1e-7).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
   python bench.py --impl reference ...   # FP64 CPU oracle on the host cores
@@ -315,29 +317,32 @@ def tuned_config(envs, batched, local, mode="auto", use=True, warm=False, precis
     return autotune.cached_single(envs[0].solver_kwargs(), device=dev, precision=precision)
 
 
-def make_solver(envs, batched, local, mode="auto", warm=None, tuned=None, precision="fp64"):
+def make_solver(envs, batched, local, mode="auto", warm=None, tuned=None, precision="fp64",
+                dx_tol=TOL, max_iter=MAX_ITER):
     if batched:
         from warpvbd_b200 import BatchedVBDSolver
-        sol = BatchedVBDSolver(envs, dx_tol=TOL, max_iter=MAX_ITER, device=f"cuda:{local}",
+        sol = BatchedVBDSolver(envs, dx_tol=dx_tol, max_iter=max_iter, device=f"cuda:{local}",
                                precision=precision, **(tuned or {}))
     else:
         from warpvbd_b200 import VBDSolver
         s = envs[0]
         shape = tuned or {"mode": mode}
-        sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=TOL,
-                        max_iter=MAX_ITER, device=f"cuda:{local}", precision=precision, **shape)
+        sol = VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, dx_tol=dx_tol,
+                        max_iter=max_iter, device=f"cuda:{local}", precision=precision, **shape)
     if warm is not None:
         sol.set_warmstart(warm)
     return sol
 
 
-def solver_for(args, envs, batched, local, warm, precision=None):
+def solver_for(args, envs, batched, local, warm, precision=None, dx_tol=TOL):
     """A solver of the workload with its tuned launch shape (and the tuned
-    shape's description)."""
+    shape's description).  A tolerance other than the workload's (the
+    accuracy reference) gets 20,000 sweeps at most."""
     precision = precision or args.precision
     tuned = tuned_config(envs, batched, local, args.mode, not args.no_tune, warm is not None,
                          precision)
-    return make_solver(envs, batched, local, args.mode, warm, tuned, precision), tuned
+    return make_solver(envs, batched, local, args.mode, warm, tuned, precision, dx_tol,
+                       MAX_ITER if dx_tol == TOL else 20000), tuned
 
 
 def warm_params(args, batched):
@@ -390,6 +395,39 @@ def timed_steps(sol, batched, steps, warmup, local, flush, sample_clocks=False, 
     clocks = clocks_stop(clk, local) if sample_clocks else None
     ms = np.array([a.elapsed_time(b) for a, b in evs])
     return ms, np.stack(iters), clocks
+
+
+def tip_displacements(sol, envs):
+    """Each environment's tip displacement (mean over its tip vertices of
+    position minus rest position), [n_env][3]."""
+    if len(envs) == 1 and not hasattr(sol, "env_slice"):
+        x = sol.old_positions.numpy()
+        e = envs[0]
+        return ((x[e.tip] - e.vertices[e.tip]).mean(0))[None, :]
+    x = sol.positions()
+    out = np.empty((len(envs), 3))
+    for i, e in enumerate(envs):
+        xe = x[sol.env_slice(i)]
+        out[i] = (xe[e.tip] - e.vertices[e.tip]).mean(0)
+    return out
+
+
+def tip_error(warm, plain, precision):
+    """Tip error of the warm-started run against the plain run at the same
+    tolerance (in fp64 the plain run is the FP64 oracle's trajectory to
+    rounding): |d_warm - d_plain| at each checkpoint over the environment's
+    largest plain tip displacement of all checkpoints.  warm / plain:
+    [checkpoints][n_env][3]."""
+    scale = np.linalg.norm(plain, axis=2).max(0)
+    rel = np.linalg.norm(warm - plain, axis=2) / scale[None, :]
+    return {"against": ("plain VBD in fp64 at the same tolerance (the FP64 oracle's "
+                        "trajectory to rounding)" if precision == "fp64" else
+                        f"plain VBD in {precision} at the same tolerance"),
+            "normalised_by": "the environment's largest plain tip displacement",
+            "max": float(rel.max()), "median": float(np.median(rel)),
+            "max_by_checkpoint": [float(v) for v in rel.max(1)],
+            "median_by_checkpoint": [float(v) for v in np.median(rel, 1)],
+            "target": 1e-4, "within_target": bool(rel.max() <= 1e-4)}
 
 
 def max_over_ranks(x, world, local):
@@ -559,10 +597,28 @@ def run_ours(args, envs, desc, batched):
         # the workload's whole trajectory from rest, plain and warm-started,
         # every step device-timed
         from warpvbd_b200 import warmstart
-        long = {}
-        for name, model in (("plain", None), ("warm_start", warmstart.load())):
-            ls, _ = solver_for(args, envs, batched, local, model)
-            lms, lit, _ = timed_steps(ls, batched, args.long_steps, 0, local, flush)
+        long, tips = {}, {}
+        for name, model, tol in (("plain", None, TOL), ("warm_start", warmstart.load(), TOL),
+                                 ("plain_tol_1e-9", None, 1e-9)):
+            if tol != TOL and args.no_accuracy_run:
+                continue
+            ls, _ = solver_for(args, envs, batched, local, model, dx_tol=tol)
+            # 100 steps at a time; each environment's tip displacement is
+            # read (untimed) between the chunks
+            chunks, tip = [], []
+            for c0 in range(0, args.long_steps, 100):
+                chunks.append(timed_steps(ls, batched, min(100, args.long_steps - c0), 0, local,
+                                          flush))
+                tip.append(tip_displacements(ls, envs))
+            lms = np.concatenate([c[0] for c in chunks])
+            lit = np.concatenate([c[1] for c in chunks])
+            tips[name] = np.stack(tip)
+            if tol != TOL:
+                # the accuracy reference: untimed figures only
+                long[name] = {"iters_per_step": {"mean": float(lit.mean()), "max": int(lit.max())},
+                              "ms_per_step": float(lms.mean())}
+                ls.close()
+                continue
             long[name] = {"ms_per_step": float(lms.mean()),
                           "iters_per_step": {"mean": float(lit.mean()), "max": int(lit.max())},
                           "value": n_env * DT / (float(lms.mean()) * 1e-3),
@@ -572,6 +628,18 @@ def run_ours(args, envs, desc, batched):
             ls.close()
         long["warm_start_speedup"] = (long["plain"]["ms_per_step"]
                                       / long["warm_start"]["ms_per_step"])
+        long["warm_start_tip_error"] = tip_error(tips["warm_start"], tips["plain"],
+                                                 args.precision)
+        if "plain_tol_1e-9" in tips:
+            # both forms against the same near-converged trajectory (plain
+            # VBD at tol 1e-9): the accuracy each buys at tol 1e-7
+            ref = tips["plain_tol_1e-9"]
+            long["tip_error_vs_tol_1e-9"] = {
+                name: {k: v for k, v in tip_error(tips[name], ref, args.precision).items()
+                       if k not in ("against", "normalised_by", "target", "within_target")}
+                for name in ("plain", "warm_start")}
+            long["tip_error_vs_tol_1e-9"]["normalised_by"] = (
+                "the environment's largest tip displacement in the tol-1e-9 run")
         line[f"batch_{args.long_steps}_steps"] = long
         if args.precision != "mixed":
             # the fp32-arithmetic mode on the same window, for comparison:
@@ -585,6 +653,22 @@ def run_ours(args, envs, desc, batched):
                 "warm_start": warm is not None}
             ms_.close()
     if rank == 0 and world == 1 and batched and not args.no_secondary:
+        # the plain single-mesh solver on the largest cantilever of the
+        # resolution sweep, 320x32x32 (349,569 vertices; from rest)
+        big = scenes.cantilever(320)
+        bs, _ = solver_for(args, [big], False, local, None)
+        bdet = {}
+        bms, bit, _ = timed_steps(bs, False, 10, 3, local, flush, detail=bdet)
+        bb, bsolved, _ = sweep_bytes(big)
+        tb = float(bms.sum()) * 1e-3
+        tbk = float(np.sum(bdet["kernel_ms"])) * 1e-3
+        line["cantilever320"] = {
+            "sim_s_per_wall_s": 10 * DT / tb, "ms_per_step": 1e3 * tb / 10,
+            "iters_per_step": float(bit.mean()), "mode": MODE_NAMES[bs.info()["mode"]],
+            "vertex_updates_per_s": bsolved * float(bit.sum()) / tb,
+            "roofline_frac": bb * float(bit.sum()) / tbk / 1e9 / peak,
+            "kernel_ms_per_step": 1e3 * tbk / 10, "steps": "4-13 from rest"}
+        bs.close()
         # the plain single-mesh solver on the 160x16x16 cantilever (from rest)
         cant = scenes.cantilever(160)
         cs, _ = solver_for(args, [cant], False, local, None)
@@ -600,20 +684,23 @@ def run_ours(args, envs, desc, batched):
             "vertex_updates_per_s": csolved * float(cit.sum()) / t,
             "roofline_frac": cb * float(cit.sum()) / tk / 1e9 / peak,
             "kernel_ms_per_step": 1e3 * tk / args.secondary_steps}
-        cs.close()
         # the same cantilever with the learned warm start (persistent mode)
         from warpvbd_b200 import warmstart
         ws_, _ = solver_for(args, [cant], False, local, warmstart.load())
         wdet = {}
         wms, wit, _ = timed_steps(ws_, False, args.secondary_steps, 3, local, flush, detail=wdet)
         tw = float(wms.sum()) * 1e-3
+        ctip = tip_error(tip_displacements(ws_, [cant])[None], tip_displacements(cs, [cant])[None],
+                         args.precision)
         line["cantilever160_warm_start"] = {
+            "tip_error_vs_plain": {k: ctip[k] for k in ("against", "max", "target")},
             "sim_s_per_wall_s": args.secondary_steps * DT / tw,
             "ms_per_step": 1e3 * tw / args.secondary_steps,
             "iters_per_step": float(wit.mean()),
             "kernel_ms_per_step": float(np.mean(wdet["kernel_ms"])),
             "speedup_vs_plain": t / tw}
         ws_.close()
+        cs.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -634,6 +721,9 @@ def main():
     ap.add_argument("--secondary-steps", type=int, default=30)
     ap.add_argument("--long-steps", type=int, default=1000,
                     help="steps of the whole-trajectory plain / warm-started batch comparison")
+    ap.add_argument("--no-accuracy-run", action="store_true",
+                    help="skip the tol-1e-9 reference trajectory of the whole-trajectory "
+                         "comparison (about 22 s on B200)")
     ap.add_argument("--start-step", type=int, default=500,
                     help="untimed steps from rest before the warm-up and timed steps")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "fp32"])
