@@ -517,6 +517,8 @@ def run_ours(args, envs, desc, batched):
                        "order_index": bool((tuned or {}).get("order_index", False)),
                        "autotuned": tuned is not None,
                        "tiered": bool((tuned or {}).get("tiered", False)),
+                       "wide_tier": bool((tuned or {}).get("tiered", False)
+                                         and (tuned or {}).get("wide_tier", True)),
                        "l2": "256 MiB written between timed steps"},
             "iters_per_step": {"hist": sweep_histogram(iters),
                                "mean": float(iters.mean()), "max": int(iters.max()),

@@ -83,6 +83,11 @@ typedef struct vbd_solver vbd_solver;
  * at the same time (block_threads threads, shared memory for the largest of
  * them, so several blocks share an SM) */
 #define VBD_TIERED 0x4000
+/* with VBD_TIERED: a third launch, beside the other two, with clusters twice
+ * the size (at most 16 blocks) for the environments the planner predicts
+ * would otherwise set the step time; the planner uses it only when its
+ * duration model says it shortens the step */
+#define VBD_TIERED_WIDE 0x80
 /* persistent mode: separate the colours of a sweep with grid barriers instead
  * of the default neighbour-scoped readiness (each block waits only for the
  * blocks owning vertices that share a tet with its own) */

@@ -268,6 +268,33 @@ def test_trained_network_reduces_sweeps():
     assert max(rel_w) < 5e-2 and np.median(rel_w) < 1e-2, rel_w
 
 
+def test_wide_tier_is_used_late_and_bit_identical():
+    """The tiered batch with the wide tier (a third launch, clusters of 8)
+    against the same batch without it, warm-started, 300 steps and then 10
+    traced: the planner puts environments on the wide tier late in the
+    trajectory, and every position is the same bit for bit (an environment's
+    arithmetic does not depend on how many blocks share it)."""
+    from warpvbd_b200 import BatchedVBDSolver
+    envs = scenes.env_batch(256, seed=0)
+    kw = dict(dx_tol=1e-7, max_iter=1000, tpv=4, block_threads=512, cluster=4, tiered=True,
+              order_index=True)
+    a = BatchedVBDSolver(envs, **kw, wide_tier=True)
+    b = BatchedVBDSolver(envs, **kw, wide_tier=False)
+    model = _trained()
+    a.set_warmstart(model)
+    b.set_warmstart(model)
+    for _ in range(300):
+        assert np.array_equal(a.step(1e-3), b.step(1e-3))
+    a.set_trace(True)
+    used = 0
+    for _ in range(10):
+        assert np.array_equal(a.step(1e-3), b.step(1e-3))
+        used += int((a.timeline()["launch"] == 2).any())
+    assert np.array_equal(a.positions(), b.positions())
+    print(f"wide tier used on {used} of 10 steps")
+    assert used > 0
+
+
 def test_warm_started_batch_is_no_less_accurate_than_plain_at_the_same_tolerance():
     """The 256-environment batch for 300 steps at tol 1e-7, plain and
     warm-started, each environment's tip displacement against a plain run at

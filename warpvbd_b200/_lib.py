@@ -44,6 +44,7 @@ MODE_HOSTLOOP = 0x300
 ORDER_INDEX = 0x1000
 STRICT_SPD = 0x2000
 TIERED = 0x4000
+TIERED_WIDE = 0x80
 PERSIST_GRID_BARRIERS = 0x8000
 CLUSTER_SHIFT = 16
 MAX_CLUSTER = 16

@@ -55,7 +55,8 @@ SINGLE_SPACE = {
     "graph": {"tpv": [4, 2, 8, 16], "order_index": [False, True]},
 }
 BATCH_SPACE = {
-    "block": {"tiered": [True, False], "cluster": [4, 8, 2, 16], "tpv": [4, 2, 8],
+    "block": {"tiered": [True, False], "wide_tier": [True, False],
+              "cluster": [4, 8, 2, 16], "tpv": [4, 2, 8],
               "block_threads": [256, 128, 512], "order_index": [False, True]},
 }
 # Shared memory a block-mode step may use (bytes), and per vertex.
@@ -252,13 +253,15 @@ def tune_single(solver_kwargs, *, material="snh", precision="fp64", device="cuda
 
 
 def tune_batched(envs, *, material="snh", precision="fp64", device="cuda", dt=1e-3,
-                 dx_tol=1e-7, max_iter=1000, steps=12, warmup=4, spaces=None, cache_path=None,
+                 dx_tol=1e-7, max_iter=1000, steps=12, warmup=300, spaces=None, cache_path=None,
                  refresh=False, verbose=False, warm=None):
     """Fastest launch shape for a batch of environments: a dict of
     BatchedVBDSolver keyword arguments (tpv, block_threads, cluster,
-    order_index).  Each candidate runs `warmup` + `steps` steps from rest: the
-    sweep counts of a batch grow over its first steps as the motion develops,
-    so a window that is too short favours the wrong shape.
+    order_index, tiered, wide_tier).  Each candidate runs `warmup` untimed
+    and `steps` timed steps from rest: the sweep counts of a batch grow over
+    its first few hundred steps as the motion develops and become uneven
+    across environments, so a window at rest favours the wrong shape (the
+    default times steps 301-312).
     With `warm` (a warm-start model, see warpvbd_b200.warmstart)
     the candidates are timed with the learned warm start on, and the result
     is cached under its own key: the warm-started sweep counts are far more
@@ -283,8 +286,8 @@ def tune_batched(envs, *, material="snh", precision="fp64", device="cuda", dt=1e
     spaces = spaces or BATCH_SPACE
 
     def evaluate(cfg):
-        args = {k: cfg[k] for k in ("tpv", "block_threads", "cluster", "order_index", "tiered")
-                if k in cfg}
+        args = {k: cfg[k] for k in ("tpv", "block_threads", "cluster", "order_index", "tiered",
+                                    "wide_tier") if k in cfg}
         try:
             sol = BatchedVBDSolver(envs, dx_tol=dx_tol, max_iter=max_iter, device=device,
                                    material=material, precision=precision, **args)
@@ -306,6 +309,7 @@ def tune_batched(envs, *, material="snh", precision="fp64", device="cuda", dt=1e
     best, cost, log = search_families(spaces, evaluate)
     cfg = {k: v for k, v in _kwargs(best).items() if k != "mode"}
     cfg["tiered"] = bool(best.get("tiered", False))
+    cfg["wide_tier"] = cfg["tiered"] and bool(best.get("wide_tier", True))
     store(key, cfg, {"ms_per_step": cost, "device": name, "evaluated": len(log),
                      "tune_s": round(time.perf_counter() - t0, 1), "n_env": len(envs),
                      "n_vertices": int(offs[-1])}, cache_path)

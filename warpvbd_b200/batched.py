@@ -25,12 +25,16 @@ class BatchedVBDSolver:
     def __init__(self, envs, damping_coefficient=0.0, gravity=(0.0, 0.0, -9.81), dx_tol=1e-7,
                  max_iter=1000, device="cuda", *, material="snh", precision="fp64",
                  tpv=0, block_threads=0, cluster=0, order_index=False, tiered=False,
-                 tune=False, gpu_setup=False):
+                 wide_tier=None, tune=False, gpu_setup=False):
         """``cluster``: blocks per thread-block cluster (0 = automatic); an
         environment much heavier than the others runs on a whole cluster.
         ``tiered``: run the environments split over a cluster in one launch
         and all others, one block each with shared memory sized for the
         largest of them, in a second launch beside it.
+        ``wide_tier`` (with ``tiered``; None = on): a third launch with
+        clusters twice that size for the environments the planner predicts
+        would otherwise set the step time (it is used only on steps where
+        the duration model says it helps; results are bit-identical).
         ``tune``: pick tpv / block_threads / cluster / order_index / tiered
         with the autotuner (warpvbd_b200.autotune; measured once, then
         cached).  ``gpu_setup``: colour all environments in one GPU pass
@@ -42,6 +46,7 @@ class BatchedVBDSolver:
             tpv, block_threads = cfg["tpv"], cfg["block_threads"]
             cluster, order_index = cfg["cluster"], cfg["order_index"]
             tiered = cfg.get("tiered", False)
+            wide_tier = cfg.get("wide_tier", wide_tier)
         self.device = device
         Xs, Ts, rho, E, nu, act = [], [], [], [], [], []
         voff, toff = [0], [0]
@@ -74,6 +79,8 @@ class BatchedVBDSolver:
             flags |= _lib.ORDER_INDEX
         if tiered:
             flags |= _lib.TIERED
+            if wide_tier is None or wide_tier:
+                flags |= _lib.TIERED_WIDE
         if gpu_setup:
             flags |= _lib.GPU_SETUP
         L = _lib.load()
@@ -111,7 +118,8 @@ class BatchedVBDSolver:
         """Timeline of the last finished traced step, one row per thread
         block: dict of arrays start_ns, end_ns (relative to the earliest
         start), env, rank (in its cluster), sm, sweeps, launch (0 the single
-        or heavy launch, 1 the light launch of a tiered step)."""
+        or split launch, 1 the light launch of a tiered step, 2 its wide
+        tier)."""
         L = _lib.load()
         n = ctypes.c_int(0)
         _lib.check(L.vbd_get_trace(self._h, None, 0, ctypes.byref(n)), "vbd_get_trace")

@@ -546,13 +546,21 @@ struct vbd_solver {
   DevBuf<int4> d_work2;
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // wide tier (VBD_TIERED_WIDE): `work3` lists the environments split over a
+  // cluster of cluster_wide blocks (third launch, stream aux2)
+  int cluster_wide = 0;
+  size_t smem_wide = 0;
+  std::vector<int4> work3;
+  DevBuf<int4> d_work3;
+  cudaStream_t aux2 = nullptr;
+  cudaEvent_t ev_join2 = nullptr;
   // timing of the step kernels of every step (events around them on the
   // solver's stream) and the number of kernels the step launched
   cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr;
   int launches_pending = 0, launches_last = 0;
   float kernel_ms_last = 0.f;
   // block-mode timeline (vbd_set_trace): 4 words per block of the step's
-  // launches, heavy / single launch first, then the light launch
+  // launches: wide tier, split (or single) launch, then the light launch
   bool trace_on = false;
   DevBuf<unsigned long long> d_trace;
   int trace_pending = 0, trace_last = 0;
@@ -647,6 +655,7 @@ void free_solver(vbd_solver* s) {
   s->d_tol.release();
   s->d_work.release();
   s->d_work2.release();
+  s->d_work3.release();
   s->d_trace.release();
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_k0) cudaEventDestroy(s->ev_k0);
@@ -655,6 +664,11 @@ void free_solver(vbd_solver* s) {
   if (s->aux) {
     cudaStreamSynchronize(s->aux);
     cudaStreamDestroy(s->aux);
+  }
+  if (s->ev_join2) cudaEventDestroy(s->ev_join2);
+  if (s->aux2) {
+    cudaStreamSynchronize(s->aux2);
+    cudaStreamDestroy(s->aux2);
   }
   s->d_wstat.release();
   s->d_chunk_owner.release();
@@ -744,13 +758,23 @@ double split_overhead(int C) {
   return v[3];
 }
 
+// With the wide tier (VBD_TIERED_WIDE, tiered mode) the longest split
+// environments may instead take a cluster of Cw = cluster_wide blocks, in a
+// third launch: the planner tries every split of the environments, longest
+// first, into h1 wide, h - h1 split over C and n - h single-block ones, and
+// keeps the one with the smallest predicted step time (the largest of the
+// longest job of each kind and the total block time / resident blocks).
 void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
-               std::vector<int4>& work2) {
+               std::vector<int4>& work2, std::vector<int4>& work3) {
   const int n = s->n_env, C = s->cluster;
+  const int Cw = s->tiered ? s->cluster_wide : 0;
   work2.clear();
+  work3.clear();
   const double a1 = 8300.0;
   const double aC = split_overhead(C);
-  std::vector<double> d1(n), dC(n), m1(n), mC(n);  // high and mean estimates
+  const double aW = Cw > 1 ? split_overhead(Cw) : 0.0;
+  // high and mean estimates on one block, on C blocks and on Cw blocks
+  std::vector<double> d1(n), dC(n), dW(n), m1(n), mC(n), mW(n);
   const bool hist = s->env_sweeps.size() == (size_t)n && s->env_sweeps_mean.size() == (size_t)n &&
                     s->env_sweeps_decay.size() == (size_t)n;
   // the learned warm start's energy checks cost about 0.7 sweeps (measured)
@@ -767,8 +791,10 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
     const double slots = s->env_work[e];
     d1[e] = k * (slots + a1);
     dC[e] = C > 1 ? k * (slots / C + aC) : d1[e];
+    dW[e] = Cw > 1 ? k * (slots / Cw + aW) : dC[e];
     m1[e] = km * (slots + a1);
     mC[e] = C > 1 ? km * (slots / C + aC) : m1[e];
+    mW[e] = Cw > 1 ? km * (slots / Cw + aW) : mC[e];
   }
   std::vector<int> order(n);
   for (int e = 0; e < n; ++e) order[e] = e;
@@ -783,28 +809,46 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
     return;
   }
   const double cap = std::max(1, s->capacity_blocks);
-  double area = 0.0;
-  for (double x : m1) area += x;
-  int best_h = 0;
-  double best_t = 1e300, t_split = 0.0;
-  for (int h = 0; h <= n; ++h) {
-    // the h longest environments are split
-    if (h > 0) {
-      const int e = order[h - 1];
-      area += C * mC[e] - m1[e];
-      t_split = std::max(t_split, dC[e]);
+  double area0 = 0.0;
+  for (double x : m1) area0 += x;
+  int best_h1 = 0, best_h = 0;
+  double best_t = 1e300;
+  double t_wide = 0.0;
+  // h1: the longest environments on a wide cluster (none without the tier)
+  for (int h1 = 0; h1 <= (Cw > 1 ? n : 0); ++h1) {
+    if (h1 > 0) {
+      const int e = order[h1 - 1];
+      area0 += Cw * mW[e] - m1[e];
+      t_wide = std::max(t_wide, dW[e]);
     }
-    const double t_single = h < n ? d1[order[h]] : 0.0;
-    const double t = std::max(std::max(t_split, t_single), area / cap);
-    if (t < best_t * 0.999) {
-      best_t = t;
-      best_h = h;
+    double area = area0, t_split = 0.0;
+    for (int h = h1; h <= n; ++h) {
+      // environments h1 .. h-1 are split over C blocks
+      if (h > h1) {
+        const int e = order[h - 1];
+        area += C * mC[e] - m1[e];
+        t_split = std::max(t_split, dC[e]);
+      }
+      const double t_single = h < n ? d1[order[h]] : 0.0;
+      const double t = std::max(std::max(std::max(t_wide, t_split), t_single), area / cap);
+      if (t < best_t * 0.999) {
+        best_t = t;
+        best_h1 = h1;
+        best_h = h;
+      }
+      if (t_single <= std::max(t_split, t_wide)) break;  // splitting more cannot help
     }
-    if (t_single <= t_split) break;  // splitting more cannot help
+    // a wider cluster for the next environment cannot beat this once the
+    // wide jobs alone are the longest
+    if (h1 < n && t_wide >= best_t) break;
   }
-  std::stable_sort(order.begin(), order.begin() + best_h,
+  std::stable_sort(order.begin(), order.begin() + best_h1,
+                   [&](int a, int b) { return dW[a] > dW[b]; });
+  std::stable_sort(order.begin() + best_h1, order.begin() + best_h,
                    [&](int a, int b) { return dC[a] > dC[b]; });
-  for (int i = 0; i < best_h; ++i)
+  for (int i = 0; i < best_h1; ++i)
+    for (int r = 0; r < Cw; ++r) work3.push_back(make_int4(order[i], r, Cw, 2));
+  for (int i = best_h1; i < best_h; ++i)
     for (int r = 0; r < C; ++r) work.push_back(make_int4(order[i], r, C, 0));
   if (s->tiered) {
     // the others run one block each in the light launch
@@ -830,13 +874,13 @@ size_t tier_smem(const vbd_solver* s, const std::vector<int4>& w) {
 }
 
 int upload_plan(vbd_solver* s, const int* iters) {
-  std::vector<int4> w, w2;
-  make_plan(s, iters, w, w2);
-  const bool same = w.size() == s->work.size() && w2.size() == s->work2.size() &&
-                    std::memcmp(w.data(), s->work.data(), w.size() * sizeof(int4)) == 0 &&
-                    std::memcmp(w2.data(), s->work2.data(), w2.size() * sizeof(int4)) == 0;
-  if (same) return VBD_OK;
-  if (w.size() > s->d_work.n || w2.size() > s->d_work2.n)
+  std::vector<int4> w, w2, w3;
+  make_plan(s, iters, w, w2, w3);
+  auto same_as = [](const std::vector<int4>& a, const std::vector<int4>& b) {
+    return a.size() == b.size() && std::memcmp(a.data(), b.data(), a.size() * sizeof(int4)) == 0;
+  };
+  if (same_as(w, s->work) && same_as(w2, s->work2) && same_as(w3, s->work3)) return VBD_OK;
+  if (w.size() > s->d_work.n || w2.size() > s->d_work2.n || w3.size() > s->d_work3.n)
     return fail(VBD_ERR_CUDA, "work map larger than its buffer");
   // the streams are idle here (create, or after a synchronising step)
   if (!w.empty())
@@ -844,11 +888,16 @@ int upload_plan(vbd_solver* s, const int* iters) {
   if (!w2.empty())
     CUDA_TRY(
         cudaMemcpy(s->d_work2.p, w2.data(), w2.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  if (!w3.empty())
+    CUDA_TRY(
+        cudaMemcpy(s->d_work3.p, w3.data(), w3.size() * sizeof(int4), cudaMemcpyHostToDevice));
   s->work.swap(w);
   s->work2.swap(w2);
+  s->work3.swap(w3);
   if (s->tiered) {
     s->smem_heavy = tier_smem(s, s->work);
     s->smem_light = tier_smem(s, s->work2);
+    s->smem_wide = tier_smem(s, s->work3);
   }
   return VBD_OK;
 }
@@ -1009,6 +1058,11 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
   s->cluster = !block_mode ? 1 : (cl ? cl : (s->n_env > 1 ? 4 : (V > 512 ? 8 : 1)));
   s->replan = block_mode && s->n_env > 1 && s->cluster > 1;
   s->tiered = s->replan && (flags & VBD_TIERED) != 0;
+  // the wide tier: clusters twice the size of the split environments' (at
+  // most 16 blocks)
+  s->cluster_wide = s->tiered && (flags & VBD_TIERED_WIDE) && s->cluster < 16
+                        ? std::min(16, 2 * s->cluster)
+                        : 0;
   if (threads == 0)
     threads = block_mode ? (s->n_env > 1 ? 256 : 512) : (mode == VBD_MODE_PERSIST ? 128 : 256);
   if (mode == VBD_MODE_GRAPH || mode == VBD_MODE_HOSTLOOP) threads = 256;
@@ -1244,6 +1298,11 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
                    bad(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "event")))
         err = 1;
       if (!err && bad(s->d_work2.alloc((size_t)s->n_env), "work")) err = 1;
+      if (!err && s->cluster_wide > 0 &&
+          (bad(cudaStreamCreateWithFlags(&s->aux2, cudaStreamNonBlocking), "stream") ||
+           bad(cudaEventCreateWithFlags(&s->ev_join2, cudaEventDisableTiming), "event") ||
+           bad(s->d_work3.alloc((size_t)s->n_env * s->cluster_wide), "work")))
+        err = 1;
     } else {
       if (bad(env_occupancy(s->prec, s->material, s->fmt, s->tpv, s->threads, s->smem_bytes,
                             s->cluster, &occ),
@@ -1395,27 +1454,44 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
       CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, s->cur_params, dtol,
                                s->d_work.p, (int)s->work.size(), s->cluster, s->smem_bytes, st));
     } else {
-      // heavy launch first (its clusters need whole groups of free SMs), the
-      // light launch beside it on the second stream, joined before the end
-      const bool two = !s->work.empty() && !s->work2.empty();
-      launches += (s->work.empty() ? 0 : 1) + (s->work2.empty() ? 0 : 1);
-      if (two) CUDA_TRY(cudaEventRecord(s->ev_fork, st));
-      if (!s->work.empty())
-        CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->heavy_threads, m,
-                                 s->cur_params, dtol, s->d_work.p, (int)s->work.size(),
-                                 s->cluster, s->smem_heavy, st));
-      if (!s->work2.empty()) {
-        cudaStream_t ls = two ? s->aux : st;
-        if (two) CUDA_TRY(cudaStreamWaitEvent(ls, s->ev_fork, 0));
+      // the launches with the widest clusters first (they need whole groups
+      // of free SMs): wide tier, split environments, then the single-block
+      // ones; the first non-empty one on the solver's stream, the others on
+      // their own streams beside it, joined before the end.  Trace records
+      // follow the same order.
+      struct Tier {
+        const std::vector<int4>* w;
+        const int4* dw;
+        int cluster, threads;
+        size_t smem;
+      };
+      const Tier tiers[3] = {
+          {&s->work3, s->d_work3.p, s->cluster_wide, s->heavy_threads, s->smem_wide},
+          {&s->work, s->d_work.p, s->cluster, s->heavy_threads, s->smem_heavy},
+          {&s->work2, s->d_work2.p, 1, s->threads, s->smem_light}};
+      // second and third launch: streams aux and aux2 (aux2 exists with the
+      // wide tier, the only way to have three)
+      const cudaStream_t side[2] = {s->aux, s->aux2};
+      const cudaEvent_t side_join[2] = {s->ev_join, s->ev_join2};
+      int nonempty = 0;
+      for (const Tier& t : tiers) nonempty += t.w->empty() ? 0 : 1;
+      launches += nonempty;
+      if (nonempty > 1) CUDA_TRY(cudaEventRecord(s->ev_fork, st));
+      int k = -1;  // launches so far, minus one
+      size_t trace_off = 0;
+      for (const Tier& t : tiers) {
+        if (t.w->empty()) continue;
+        cudaStream_t ts = k < 0 ? st : side[k];
+        if (k >= 0) CUDA_TRY(cudaStreamWaitEvent(ts, s->ev_fork, 0));
         StepParams lp = s->cur_params;
-        if (lp.trace) lp.trace += 4 * s->work.size();
-        CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, s->threads, m, lp, dtol,
-                                 s->d_work2.p, (int)s->work2.size(), 1, s->smem_light, ls));
-        if (two) {
-          CUDA_TRY(cudaEventRecord(s->ev_join, ls));
-          CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
-        }
+        if (lp.trace) lp.trace += 4 * trace_off;
+        CUDA_TRY(launch_env_step(s->prec, s->material, s->tpv, t.threads, m, lp, dtol, t.dw,
+                                 (int)t.w->size(), t.cluster, t.smem, ts));
+        if (k >= 0) CUDA_TRY(cudaEventRecord(side_join[k], ts));
+        ++k;
+        trace_off += t.w->size();
       }
+      for (int j = 0; j < k; ++j) CUDA_TRY(cudaStreamWaitEvent(st, side_join[j], 0));
     }
   } else if (s->mode == VBD_MODE_PERSIST) {
     if (s->warm) {
@@ -1463,7 +1539,7 @@ int enqueue_step(vbd_solver* s, double dt, double tol, const double* tol_env, in
   CUDA_TRY(cudaEventRecord(s->ev_k1, st));
   s->launches_pending = launches;
   s->trace_pending = s->cur_params.trace && s->mode == VBD_MODE_BLOCK
-                         ? (int)(s->work.size() + s->work2.size())
+                         ? (int)(s->work.size() + s->work2.size() + s->work3.size())
                          : 0;
   s->pending = true;
   s->ws_history = true;  // ut now holds this step's inertia target
@@ -1669,7 +1745,7 @@ int vbd_set_trace(vbd_solver* s, int enable) {
   DeviceGuard dg(s->device);
   if (enable && !s->d_trace.p) {
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    CUDA_TRY(s->d_trace.alloc(4 * (s->d_work.n + s->d_work2.n)));
+    CUDA_TRY(s->d_trace.alloc(4 * (s->d_work.n + s->d_work2.n + s->d_work3.n)));
     CUDA_TRY(cudaMemset(s->d_trace.p, 0, sizeof(unsigned long long) * s->d_trace.n));
   }
   s->trace_on = enable != 0;
@@ -1847,7 +1923,7 @@ int vbd_get_info(vbd_solver* s, vbd_info_t* info) {
   info->last_step_launches = s->launches_last;
   info->last_step_kernel_ms = s->kernel_ms_last;
   info->n_blocks = s->mode == VBD_MODE_PERSIST ? s->persist_blocks
-                                                : (int)(s->work.size() + s->work2.size());
+                                                : (int)(s->work.size() + s->work2.size() + s->work3.size());
   return VBD_OK;
 }
 
