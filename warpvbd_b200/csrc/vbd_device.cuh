@@ -345,6 +345,65 @@ struct Prefetch {
   static constexpr int steps = (20 + TPV - 1) / TPV;
 };
 
+// The vertex's update from its summed elastic gradient g and Hessian h (the
+// lane that holds them): inertia term, damping, guarded 3x3 Newton step,
+// store, convergence measure.
+template <typename Real, typename SReal, class State>
+__device__ __forceinline__ void finish_vertex(const DevMesh& m, int gv, int lv,
+                                              const real4<SReal>& uo, const real4<SReal>& tt,
+                                              const Real (&g)[3], Real (&h)[6], const State& st,
+                                              const StepConst& sc, unsigned long long& cmax,
+                                              unsigned& stat, unsigned long long* dxrec) {
+  using S4 = real4<SReal>;
+  const Real mdt2 = Real(tt.w * SReal(sc.inv_dt2));
+  Real G[3], H[6];
+  G[0] = g[0] + mdt2 * Real(uo.x - tt.x);
+  G[1] = g[1] + mdt2 * Real(uo.y - tt.y);
+  G[2] = g[2] + mdt2 * Real(uo.z - tt.z);
+  if (sc.damp) {
+    // Rayleigh-like damping kd * H_el (x - x_prev) / dt (vbd_solver.py:222-223)
+    const S4 u0 = ldcg4(reinterpret_cast<const S4*>(m.up) + gv);
+    const Real kd = Real(sc.kd_dt);
+    const Real ex = Real(uo.x - u0.x), ey = Real(uo.y - u0.y), ez = Real(uo.z - u0.z);
+    G[0] += kd * (h[0] * ex + h[1] * ey + h[2] * ez);
+    G[1] += kd * (h[1] * ex + h[3] * ey + h[4] * ez);
+    G[2] += kd * (h[2] * ex + h[4] * ey + h[5] * ez);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) h[i] *= (Real(1) + kd);
+  }
+  H[0] = h[0] + mdt2;
+  H[1] = h[1];
+  H[2] = h[2];
+  H[3] = h[3] + mdt2;
+  H[4] = h[4];
+  H[5] = h[5] + mdt2;
+  Real dx[3];
+  if (!chol_solve3<Real>(H, G, dx)) {
+    stat |= kStatGuard;
+    if (!sc.strict) {
+      // fallback: inertia-only Hessian (m/dt^2) I; a massless vertex stays
+      const Real s = mdt2 > Real(0) ? Real(-1) / mdt2 : Real(0);
+      dx[0] = G[0] * s;
+      dx[1] = G[1] * s;
+      dx[2] = G[2] * s;
+    }
+  }
+  S4 un = uo;
+  un.x += SReal(dx[0]);
+  un.y += SReal(dx[1]);
+  un.z += SReal(dx[2]);
+  st.store(lv, un);
+  const double c = fabs(double(dx[0] + dx[1] + dx[2]));
+  if (!isfinite(c)) stat |= kStatNonFinite;
+  const unsigned long long cb = conv_bits(c);
+  cmax = cb > cmax ? cb : cmax;
+  // the last sweep allowed: its largest |dx| component, for the
+  // non-convergence report
+  if (dxrec)
+    atomicMax(dxrec, conv_bits(fmax(fabs(double(dx[0])),
+                                    fmax(fabs(double(dx[1])), fabs(double(dx[2]))))));
+}
+
 // ---------------------------------------------------------------------------
 // One warp processes one chunk (32/TPV vertices of one colour).  `st` reads
 // and writes the environment's displacements by environment-local id.
@@ -431,55 +490,142 @@ __device__ __forceinline__ void process_chunk(const DevMesh& m, int vbase, const
 #pragma unroll
     for (int i = 0; i < 6; ++i) h[i] += __shfl_xor_sync(0xffffffffu, h[i], off);
   }
-  if (valid && !vbad && sub == 0) {
-    const Real mdt2 = Real(tt.w * SReal(sc.inv_dt2));
-    Real G[3], H[6];
-    G[0] = g[0] + mdt2 * Real(uo.x - tt.x);
-    G[1] = g[1] + mdt2 * Real(uo.y - tt.y);
-    G[2] = g[2] + mdt2 * Real(uo.z - tt.z);
-    if (sc.damp) {
-      // Rayleigh-like damping kd * H_el (x - x_prev) / dt (vbd_solver.py:222-223)
-      const S4 u0 = ldcg4(reinterpret_cast<const S4*>(m.up) + gv);
-      const Real kd = Real(sc.kd_dt);
-      const Real ex = Real(uo.x - u0.x), ey = Real(uo.y - u0.y), ez = Real(uo.z - u0.z);
-      G[0] += kd * (h[0] * ex + h[1] * ey + h[2] * ez);
-      G[1] += kd * (h[1] * ex + h[3] * ey + h[4] * ez);
-      G[2] += kd * (h[2] * ex + h[4] * ey + h[5] * ez);
-#pragma unroll
-      for (int i = 0; i < 6; ++i) h[i] *= (Real(1) + kd);
-    }
-    H[0] = h[0] + mdt2;
-    H[1] = h[1];
-    H[2] = h[2];
-    H[3] = h[3] + mdt2;
-    H[4] = h[4];
-    H[5] = h[5] + mdt2;
-    Real dx[3];
-    if (!chol_solve3<Real>(H, G, dx)) {
-      stat |= kStatGuard;
-      if (!sc.strict) {
-        // fallback: inertia-only Hessian (m/dt^2) I; a massless vertex stays
-        const Real s = mdt2 > Real(0) ? Real(-1) / mdt2 : Real(0);
-        dx[0] = G[0] * s;
-        dx[1] = G[1] * s;
-        dx[2] = G[2] * s;
-      }
-    }
-    S4 un = uo;
-    un.x += SReal(dx[0]);
-    un.y += SReal(dx[1]);
-    un.z += SReal(dx[2]);
-    st.store(lv, un);
-    const double c = fabs(double(dx[0] + dx[1] + dx[2]));
-    if (!isfinite(c)) stat |= kStatNonFinite;
-    const unsigned long long cb = conv_bits(c);
-    cmax = cb > cmax ? cb : cmax;
-    // the last sweep allowed: its largest |dx| component, for the
-    // non-convergence report
-    if (dxrec)
-      atomicMax(dxrec, conv_bits(fmax(fabs(double(dx[0])),
-                                      fmax(fabs(double(dx[1])), fabs(double(dx[2]))))));
+  if (valid && !vbad && sub == 0)
+    finish_vertex<Real, SReal>(m, gv, lv, uo, tt, g, h, st, sc, cmax, stat, dxrec);
+}
+
+// ---------------------------------------------------------------------------
+// Split chunks (block mode).  A colour with fewer chunks than a block has
+// warps (kSplitWarps) leaves most warps idle while each busy lane walks all
+// of its vertex's slot steps in sequence -- at 2 lanes per vertex up to 10
+// dependent FP64 slot evaluations, ~6 us for a 3-vertex colour.  Such a
+// colour instead gives each chunk W = split_ways(chunks) warps: part p of W
+// takes the slot steps s = p, p + W, ...; each part's per-vertex sums (after
+// the lanes-per-vertex shuffle) go to shared memory, and after a barrier one
+// warp per chunk adds the W parts in part order and updates the vertices.
+// W depends only on the colour's chunk count, so the arithmetic is the same
+// whatever the block size or the number of blocks sharing the environment.
+// ---------------------------------------------------------------------------
+constexpr int kSplitWarps = 16;  // chunks x parts per colour at most
+
+template <int TPV>
+__device__ __forceinline__ int split_ways(int chunks) {
+  if (chunks <= 0 || chunks * 2 > kSplitWarps) return 1;
+  const int w = kSplitWarps / chunks;
+  return w < Prefetch<TPV>::steps ? w : Prefetch<TPV>::steps;
+}
+
+// Floats (Real) of the per-part sums of one part: 9 per vertex of a chunk.
+template <int TPV>
+struct SplitBuf {
+  static constexpr int per_part = 9 * (32 / TPV);
+};
+
+// Part `part` of `W` of chunk q: the slot steps s = part, part + W, ...
+// summed per vertex and written to buf[9 * vertex-in-chunk + i] (g then h).
+template <typename Real, typename SReal, int TPV, int MAT, int FMT, class State>
+__device__ __forceinline__ void process_chunk_part(const DevMesh& m, int vbase,
+                                                   const ColorInfo& ci, int q, int lane,
+                                                   const State& st, unsigned& stat,
+                                                   const real4<Real>* tab, int part, int W,
+                                                   Real* buf) {
+  using R4 = real4<Real>;
+  using S4 = real4<SReal>;
+  constexpr int CPW = 32 / TPV;
+  const int vi = lane / TPV, sub = lane % TPV;
+  const int gv = ci.vbegin + (q - ci.chunk_begin) * CPW + vi;
+  const bool valid = gv < ci.vend;
+  const int lv = gv - vbase;
+  const ChunkInfo ch = m.chunk[q];
+  const size_t base = (size_t)ch.block * 32 + lane;
+#if VBD_CHECK_BOUNDS
+  const EnvInfo eb = m.env[m.chunk_owner[q].y];
+  const bool vbad = valid && (lv < 0 || lv >= eb.nsolved);
+  if (vbad) stat |= kStatBounds;
+#else
+  constexpr bool vbad = false;
+#endif
+  int k = 0;
+  S4 uo;
+  uo.x = uo.y = uo.z = uo.w = SReal(0);
+  if (valid && !vbad) {
+    k = __ldg(m.valence + gv);
+    uo = st.load(lv);
   }
+  Real g[3] = {Real(0), Real(0), Real(0)};
+  Real h[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
+  for (int s = part; s < ch.steps; s += W) {
+    if (s * TPV + sub >= k) continue;
+    const int4 id = load_slot<FMT>(m, base + (size_t)s * 32);
+#if VBD_CHECK_BOUNDS
+    if ((unsigned)id.x >= (unsigned)eb.nv || (unsigned)id.y >= (unsigned)eb.nv ||
+        (unsigned)id.z >= (unsigned)eb.nv || (unsigned)id.w >= (unsigned)eb.nrec) {
+      stat |= kStatBounds;
+      continue;
+    }
+#endif
+    const R4* t = tab + 3 * (size_t)id.w;
+    const R4 q0 = t[0];
+    const R4 q1 = t[1];
+    const R4 q2 = t[2];
+    const S4 a = st.load(id.x);
+    const S4 b = st.load(id.y);
+    const S4 c = st.load(id.z);
+    slot_accumulate<Real, MAT>(Real(a.x - uo.x), Real(a.y - uo.y), Real(a.z - uo.z),
+                               Real(b.x - uo.x), Real(b.y - uo.y), Real(b.z - uo.z),
+                               Real(c.x - uo.x), Real(c.y - uo.y), Real(c.z - uo.z), q0, q1, q2,
+                               g, h);
+  }
+#pragma unroll
+  for (int off = TPV / 2; off > 0; off >>= 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) g[i] += __shfl_xor_sync(0xffffffffu, g[i], off);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) h[i] += __shfl_xor_sync(0xffffffffu, h[i], off);
+  }
+  if (sub == 0) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) buf[9 * vi + i] = g[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) buf[9 * vi + 3 + i] = h[i];
+  }
+}
+
+// Chunk q after its W parts are in parts[w * SplitBuf<TPV>::per_part + ...]:
+// the sums in part order, then the vertex updates.
+template <typename Real, typename SReal, int TPV, class State>
+__device__ __forceinline__ void finish_split_chunk(const DevMesh& m, int vbase,
+                                                   const ColorInfo& ci, int q, int lane,
+                                                   const State& st, const StepConst& sc,
+                                                   unsigned long long& cmax, unsigned& stat,
+                                                   unsigned long long* dxrec, const Real* parts,
+                                                   int W) {
+  using S4 = real4<SReal>;
+  constexpr int CPW = 32 / TPV;
+  if (lane >= CPW) return;  // one lane per vertex
+  const int vi = lane;
+  const int gv = ci.vbegin + (q - ci.chunk_begin) * CPW + vi;
+  if (gv >= ci.vend) return;
+  const int lv = gv - vbase;
+#if VBD_CHECK_BOUNDS
+  const EnvInfo eb = m.env[m.chunk_owner[q].y];
+  if (lv < 0 || lv >= eb.nsolved) return;  // reported by the parts
+#endif
+  Real g[3], h[6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) g[i] = parts[9 * vi + i];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) h[i] = parts[9 * vi + 3 + i];
+  for (int w = 1; w < W; ++w) {
+    const Real* p = parts + w * SplitBuf<TPV>::per_part + 9 * vi;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) g[i] += p[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) h[i] += p[3 + i];
+  }
+  const S4 uo = st.load(lv);
+  const S4 tt = ldcg4(reinterpret_cast<const S4*>(m.ut) + gv);
+  finish_vertex<Real, SReal>(m, gv, lv, uo, tt, g, h, st, sc, cmax, stat, dxrec);
 }
 
 // ---------------------------------------------------------------------------

@@ -96,17 +96,37 @@ __device__ __forceinline__ int env_sweeps(const DevMesh& m, const EnvInfo& e, co
                                           unsigned long long* s_red,
                                           unsigned long long (*s_conv)[kMaxGroup],
                                           int* s_done, const real4<Real>* tab,
-                                          unsigned long long* dxw) {
+                                          unsigned long long* dxw, Real* s_split) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  constexpr int kPart = SplitBuf<TPV>::per_part;
   int it = 0;
   for (;;) {
     unsigned long long cmax = 0ull;
     unsigned long long* dxrec = it + 1 == max_iter ? dxw : nullptr;
     for (int c = 0; c < e.ncolors; ++c) {
       const ColorInfo ci = m.color[e.cbase + c];
-      for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
-        process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, su, sc, cmax, stat,
-                                                  tab, dxrec);
+      const int nch = ci.chunk_end - ci.chunk_begin;
+      const int W = split_ways<TPV>(nch);
+      if (W == 1) {
+        for (int q = ci.chunk_begin + rank + g * warp; q < ci.chunk_end; q += g * nwarps)
+          process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, su, sc, cmax, stat,
+                                                    tab, dxrec);
+      } else {
+        // this block's chunks rank, rank + g, ...; W parts each (nloc x W <=
+        // kSplitWarps, the size of s_split)
+        const int nloc = rank < nch ? (nch - rank + g - 1) / g : 0;
+        for (int pi = warp; pi < nloc * W; pi += nwarps) {
+          const int q = ci.chunk_begin + rank + g * (pi / W);
+          process_chunk_part<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, su, stat, tab,
+                                                         pi % W, W, s_split + pi * kPart);
+        }
+        __syncthreads();
+        for (int kl = warp; kl < nloc; kl += nwarps)
+          finish_split_chunk<Real, SReal, TPV>(m, e.vbase, ci, ci.chunk_begin + rank + g * kl,
+                                               lane, su, sc, cmax, stat, dxrec,
+                                               s_split + kl * W * kPart, W);
+        // s_split is reused by the next colour after the barrier below
+      }
       group_sync<GROUP>(g);
     }
     ++it;
@@ -301,6 +321,8 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
   __shared__ double2 s_pair[kMaxGroup];
   __shared__ int s_done;
   __shared__ unsigned s_stat;
+  // per-part sums of the split chunks of small colours (env_sweeps)
+  __shared__ Real s_split[kSplitWarps * SplitBuf<TPV>::per_part];
   const int4 w = work[blockIdx.x];
   const int env = w.x, rank = w.y, g = w.z;
   if (env < 0) return;  // padding block of a cluster of single-block environments
@@ -339,7 +361,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, GROUP>(m, e, su, rank, g, sc, p.max_iter, tol,
                                                         stat, converged, s_red, s_conv, &s_done,
-                                                        tab, m.dxmax + env);
+                                                        tab, m.dxmax + env, s_split);
   } else {
     __syncthreads();
     if (p.warm && m.ws_pred) {
@@ -349,7 +371,7 @@ __global__ void __launch_bounds__(512) env_step_kernel(DevMesh m, StepParams p,
     }
     it = env_sweeps<Real, SReal, TPV, MAT, FMT, false>(m, e, local, 0, 1, sc, p.max_iter, tol,
                                                         stat, converged, s_red, s_conv, &s_done,
-                                                        tab, m.dxmax + env);
+                                                        tab, m.dxmax + env, s_split);
   }
   // velocity update and write-back, vertices split over the group
   for (int i = rank + g * threadIdx.x; i < e.nv; i += g * blockDim.x) {
@@ -521,7 +543,10 @@ __global__ void zero_xyz_kernel(real4<Real>* st, int n) {
 // ---------------------------------------------------------------------------
 namespace {
 // opt-in limit is 227 KB per block including the kernel's static shared memory
-constexpr int kMaxSmem = 227 * 1024 - 2048;
+// dynamic shared memory of a block-mode block at most: 227 KB less the
+// kernel's static arrays (2 KB of reductions, and the split-chunk sums: 16
+// parts x 9 values x 16 vertices x 8 bytes at the largest)
+constexpr int kMaxSmem = 227 * 1024 - 2048 - kSplitWarps * 9 * 16 * 8;
 
 template <typename Real, typename SReal, int TPV, int MAT, int FMT, bool GROUP>
 cudaError_t configure_env_kernel() {
