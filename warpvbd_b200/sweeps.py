@@ -4,9 +4,10 @@ tolerance study behind benchmark_accuracy_tolerance.png).
 
     python -m warpvbd_b200.sweeps --out sweeps.json [--quick]
 
-Every result carries its error against an FP64 run of the same solver on the
-same mesh, material, tolerance and steps (precision="fp64": identical
-algorithm, fp64 state and arithmetic).
+Every row times the default solver (precision="fp64", the reference's
+precision) and the fp32-arithmetic mode (precision="mixed") on the same mesh,
+material, tolerance and steps, and gives the mixed run's error against the
+FP64 one.
 
 - resolution   cantilever 20x2x2 ... 320x32x32 (beam 1.0 x 0.1 x 0.1 m,
                x = 0 face fixed), Stable Neo-Hookean and St. Venant-Kirchhoff,
@@ -41,27 +42,33 @@ def _solver(s, **kw):
     from .vbd_solver import VBDSolver
     kw.setdefault("dx_tol", 1e-7)
     kw.setdefault("max_iter", 1000)
+    kw.setdefault("tune", True)  # the autotuned launch shape (cached per mesh and precision)
     return VBDSolver(**s.solver_kwargs(), damping_coefficient=0.0, **kw)
 
 
 def _pair_run(s, steps, dt=1e-3, tol=1e-7, material="snh", mode="auto", ref_tol=None,
               max_iter=1000, record=None):
     """Step the mixed-precision solver and its FP64 twin together; returns a
-    dict of errors, sweeps and timing (timing of the mixed run only)."""
+    dict of the mixed run's errors against the FP64 run, and sweeps and
+    timing of both (wall time of each step with its positions download)."""
     import torch
-    a = _solver(s, dx_tol=tol, material=material, mode=mode, max_iter=max_iter)
-    b = _solver(s, dx_tol=ref_tol or tol, material=material, precision="fp64",
+    a = _solver(s, dx_tol=tol, material=material, mode=mode, max_iter=max_iter,
+                precision="mixed")
+    b = _solver(s, dx_tol=ref_tol or tol, material=material, mode=mode, precision="fp64",
                 max_iter=max(max_iter, 20000 if ref_tol else max_iter))
     D = _diag(s.vertices)
-    worst, its, t_mixed = 0.0, [], 0.0
+    worst, its, its_b, t_mixed, t_fp64 = 0.0, [], [], 0.0, 0.0
     trace = []
     for k in range(steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         xa = a.step(a.old_positions, dt).numpy()
-        t_mixed += time.perf_counter() - t0
+        t1 = time.perf_counter()
         xb = b.step(b.old_positions, dt).numpy()
+        t_mixed += t1 - t0
+        t_fp64 += time.perf_counter() - t1
         its.append(a.last_iterations)
+        its_b.append(b.last_iterations)
         worst = max(worst, float(np.abs(xa - xb).max()) / D)
         if record is not None and k % record == 0:
             trace.append([k * dt, *((xa[s.tip] - s.vertices[s.tip]).mean(0).tolist()),
@@ -78,7 +85,12 @@ def _pair_run(s, steps, dt=1e-3, tol=1e-7, material="snh", mode="auto", ref_tol=
            "tip_displacement": da.tolist(), "tip_displacement_fp64": db.tolist(),
            "sweeps_mean": float(np.mean(its)), "sweeps_max": int(np.max(its)),
            "sim_s_per_wall_s": steps * dt / t_mixed,
-           "vertex_updates_per_s": solved * float(np.sum(its)) / t_mixed}
+           "vertex_updates_per_s": solved * float(np.sum(its)) / t_mixed,
+           "fp64_mode": {0x100: "block", 0x200: "graph", 0x300: "hostloop", 0x400: "persist"}[
+               b.info()["mode"]],
+           "fp64_sweeps_mean": float(np.mean(its_b)),
+           "fp64_sim_s_per_wall_s": steps * dt / t_fp64,
+           "fp64_vertex_updates_per_s": solved * float(np.sum(its_b)) / t_fp64}
     if record is not None:
         out["trace"] = trace
     a.close()
@@ -114,7 +126,7 @@ def tolerance(n=160, tols=(1e-5, 1e-6, 1e-7, 1e-8, 1e-9), steps=100):
     for tol in tols:
         r = _pair_run(s, steps, tol=tol)
         # replay the mixed run for the comparison with the converged trajectory
-        a = _solver(s, dx_tol=tol)
+        a = _solver(s, dx_tol=tol, precision="mixed")
         worst = 0.0
         for k in range(steps):
             xa = a.step(a.old_positions, 1e-3).numpy()
@@ -143,7 +155,7 @@ def nsim(counts=(1, 4, 16, 64, 256, 1024, 4096), steps=20, warmup=3):
     base = scenes.mass_spring(11, 20)
     res = {}
     for n in counts:
-        sol = BatchedVBDSolver([base] * n, dx_tol=1e-7, max_iter=1000, tpv=4,
+        sol = BatchedVBDSolver([base] * n, dx_tol=1e-7, max_iter=1000, tpv=2,
                                block_threads=512, cluster=4, tiered=n > 1)
         for _ in range(warmup):
             sol.step(1e-3)
