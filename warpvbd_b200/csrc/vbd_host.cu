@@ -519,6 +519,9 @@ struct vbd_solver {
   int cluster = 1;           // blocks per cluster = group size of a split environment
   bool replan = false;       // re-plan from the measured sweep counts after each step
   int capacity_blocks = 0;   // resident blocks on the device for this launch shape
+  // tiered mode: clusters of the split / wide size that can be resident at
+  // once (a cluster needs its blocks in one GPC, so fewer than blocks / size)
+  int max_clusters_split = 0, max_clusters_wide = 0;
   std::vector<double> env_work;  // incident slots per environment
   // sweeps per environment for the plan.  Plain VBD's counts change slowly
   // from step to step: env_sweeps_decay = max(last, 0.95 x previous).  The
@@ -730,14 +733,17 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
 // slot count and its sweep count (1 before the first step) with a per-sweep
 // cost model measured on B200 at 512 threads, in units of one slot visit of
 // a single block:
-//   one block              sweeps * (slots + 8300)
-//   split over C blocks    sweeps * (slots / C + I_C),
-//                          I_C = 10300 / 11200 / 12200 / 16500 for C = 2 / 4 / 8 / 16
-//                          (interpolated for the other sizes)
-// (the fixed part is the per-colour barrier and dependency chain: a
-// 7K-slot environment costs 29 us per sweep, a 44K-slot one 110 us; a
-// 68K-slot environment 129 / 77 / 49 / 36 / 36 us on 1 / 2 / 4 / 8 / 16
-// blocks).  With cluster > 1 the longest environments may each take a whole
+//   one block              sweeps * (slots + A1)
+//   split over C blocks    sweeps * (slots / C + I_C)
+//                          (I_C interpolated between C = 2, 4, 8, 16)
+// fitted to single environments of 7K, 27K and 68K slots on 1-16 blocks:
+//   mixed precision, 4 lanes per vertex: A1 = 8300, I_C = 10300 / 11200 /
+//     12200 / 16500 (1.72 ns per slot visit; the 68K-slot environment 129 /
+//     78 / 49 / 35 / 36 us per sweep on 1 / 2 / 4 / 8 / 16 blocks)
+//   fp64, 2 lanes per vertex: A1 = 10200, I_C = 12900 / 13500 / 13900 / 18000
+//     (2.34 ns per slot visit; 183 / 112 / 67 / 54 / 55 us)
+// (the fixed part is the per-colour barrier and dependency chain; at 16
+// blocks every store also goes to 15 replicas, which I_16 absorbs).  With cluster > 1 the longest environments may each take a whole
 // cluster (group = cluster); the split set is the one with the smallest
 // predicted step time, the largest of (longest split environment, longest
 // single-block environment, all block time / resident blocks).  With the
@@ -749,9 +755,11 @@ size_t env_smem(const vbd_solver* s, const EnvInfo& ei, bool with_tab) {
 // then starts first.
 // I_C of the duration model: measured at C = 2, 4, 8, 16, linear in C between
 // those points (C = 3, 5-7, 9-15).
-double split_overhead(int C) {
+double split_overhead(int C, bool fp64) {
   static const double c[4] = {2.0, 4.0, 8.0, 16.0};
-  static const double v[4] = {10300.0, 11200.0, 12200.0, 16500.0};
+  static const double vm[4] = {10300.0, 11200.0, 12200.0, 16500.0};
+  static const double vd[4] = {12900.0, 13500.0, 13900.0, 18000.0};
+  const double* v = fp64 ? vd : vm;
   if (C <= 2) return v[0];
   for (int i = 1; i < 4; ++i)
     if (C <= c[i]) return v[i - 1] + (v[i] - v[i - 1]) * (C - c[i - 1]) / (c[i] - c[i - 1]);
@@ -763,16 +771,20 @@ double split_overhead(int C) {
 // third launch: the planner tries every split of the environments, longest
 // first, into h1 wide, h - h1 split over C and n - h single-block ones, and
 // keeps the one with the smallest predicted step time (the largest of the
-// longest job of each kind and the total block time / resident blocks).
+// longest job of each kind, the total block time / resident blocks, and each
+// split tier's total / its resident clusters -- a cluster needs its blocks in
+// one GPC, so fewer clusters than blocks / size fit; with more jobs than
+// that, they run in waves).  At most as many wide jobs as wide clusters fit.
 void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
                std::vector<int4>& work2, std::vector<int4>& work3) {
   const int n = s->n_env, C = s->cluster;
   const int Cw = s->tiered ? s->cluster_wide : 0;
   work2.clear();
   work3.clear();
-  const double a1 = 8300.0;
-  const double aC = split_overhead(C);
-  const double aW = Cw > 1 ? split_overhead(Cw) : 0.0;
+  const bool f64 = s->prec == 2;
+  const double a1 = f64 ? 10200.0 : 8300.0;
+  const double aC = split_overhead(C, f64);
+  const double aW = Cw > 1 ? split_overhead(Cw, f64) : 0.0;
   // high and mean estimates on one block, on C blocks and on Cw blocks
   std::vector<double> d1(n), dC(n), dW(n), m1(n), mC(n), mW(n);
   const bool hist = s->env_sweeps.size() == (size_t)n && s->env_sweeps_mean.size() == (size_t)n &&
@@ -813,24 +825,35 @@ void make_plan(const vbd_solver* s, const int* iters, std::vector<int4>& work,
   for (double x : m1) area0 += x;
   int best_h1 = 0, best_h = 0;
   double best_t = 1e300;
-  double t_wide = 0.0;
-  // h1: the longest environments on a wide cluster (none without the tier)
-  for (int h1 = 0; h1 <= (Cw > 1 ? n : 0); ++h1) {
+  double t_wide = 0.0, sum_wide = 0.0;
+  // clusters resident at once (tiered mode; 0 = not known): more split jobs
+  // than that run in waves, which the per-tier sums over the resident
+  // clusters bound from below
+  const int max_w = s->max_clusters_wide, max_c = s->max_clusters_split;
+  // h1: the longest environments on a wide cluster (none without the tier,
+  // and never more than can be resident at once)
+  for (int h1 = 0; h1 <= (Cw > 1 ? std::min(n, max_w) : 0); ++h1) {
     if (h1 > 0) {
       const int e = order[h1 - 1];
       area0 += Cw * mW[e] - m1[e];
       t_wide = std::max(t_wide, dW[e]);
+      sum_wide += mW[e];
     }
-    double area = area0, t_split = 0.0;
+    // clusters of C that still fit beside the wide ones
+    const int c_free = max_c > 0 ? std::max(1, (max_c * C - h1 * Cw) / C) : 0;
+    double area = area0, t_split = 0.0, sum_split = 0.0;
     for (int h = h1; h <= n; ++h) {
       // environments h1 .. h-1 are split over C blocks
       if (h > h1) {
         const int e = order[h - 1];
         area += C * mC[e] - m1[e];
         t_split = std::max(t_split, dC[e]);
+        sum_split += mC[e];
       }
       const double t_single = h < n ? d1[order[h]] : 0.0;
-      const double t = std::max(std::max(std::max(t_wide, t_split), t_single), area / cap);
+      double t = std::max(std::max(std::max(t_wide, t_split), t_single), area / cap);
+      if (max_w > 0) t = std::max(t, sum_wide / max_w);
+      if (c_free > 0) t = std::max(t, sum_split / c_free);
       if (t < best_t * 0.999) {
         best_t = t;
         best_h1 = h1;
@@ -1293,6 +1316,18 @@ int create_impl(const double* X, int V, const int32_t* tets, int T, const double
               "occupancy"))
         err = 1;
       s->capacity_blocks = occ * sms;
+      int occ_c = 0, occ_w = 0;
+      if (!err && bad(env_occupancy(s->prec, s->material, s->fmt, s->tpv, s->heavy_threads,
+                                    s->smem_bytes, s->cluster, &occ_c),
+                      "occupancy"))
+        err = 1;
+      if (!err && s->cluster_wide > 0 &&
+          bad(env_occupancy(s->prec, s->material, s->fmt, s->tpv, s->heavy_threads,
+                            s->smem_bytes, s->cluster_wide, &occ_w),
+              "occupancy"))
+        err = 1;
+      s->max_clusters_split = occ_c;
+      s->max_clusters_wide = occ_w;
       if (!err && (bad(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking), "stream") ||
                    bad(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming), "event") ||
                    bad(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "event")))
