@@ -448,6 +448,9 @@ def run_ours(args, envs, desc, batched):
     sol, tuned = solver_for(args, envs, batched, local, warm)
     info = sol.info()
     advance(sol, batched, args.start_step)
+    # the state at the start of the window, so that the end-to-end run below
+    # covers the same steps
+    snap = (sol.positions(), sol.velocities()) if batched else sol.get_state()
     if world > 1:
         torch.distributed.barrier()
     detail = {}
@@ -458,28 +461,34 @@ def run_ours(args, envs, desc, batched):
     value = world * n_env * args.steps * DT / (total_ms * 1e-3)
 
     # end to end through the public API: every step uploads the positions
-    # from page-locked host memory and downloads the new ones into it
+    # from page-locked host memory and downloads the new ones into it.  The
+    # run restarts from the window's first state and takes the same warm-up
+    # and timed steps, so it covers the same part of the trajectory as
+    # `value` (wall clock around the timed steps, max over ranks)
     n_vertices = sum(e.n_vertices for e in envs)
+    e2e_steps = args.e2e_steps or args.steps
     xh = torch.empty((n_vertices, 3), dtype=torch.float64, pin_memory=True).numpy()
-    # (three untimed round trips first, as for the device-timed steps)
+    sol.set_state(positions=snap[0], velocities=snap[1])
+    xh[:] = snap[0]
+    if world > 1:
+        torch.distributed.barrier()
     if batched:
         # step(out=...) : the step kernels write each environment's positions
         # into the page-locked array as it finishes
-        sol.positions(out=xh)
-        for k in range(3 + args.e2e_steps):
-            if k == 3:
+        for k in range(args.warmup + e2e_steps):
+            if k == args.warmup:
                 t0 = time.perf_counter()
             sol.set_state(positions=xh)
             sol.step(DT, out=xh)
         e2e_s = time.perf_counter() - t0
     else:
-        sol.old_positions.numpy(out=xh)
-        for k in range(3 + args.e2e_steps):
-            if k == 3:
+        for k in range(args.warmup + e2e_steps):
+            if k == args.warmup:
                 t0 = time.perf_counter()
             sol.step(xh, DT).numpy(out=xh)
         e2e_s = time.perf_counter() - t0
-    e2e = world * n_env * args.e2e_steps * DT / e2e_s
+    e2e_s = max_over_ranks(e2e_s, world, local)
+    e2e = world * n_env * e2e_steps * DT / e2e_s
 
     # roofline of the dominant kernel: algorithmic bytes of the sweeps it ran
     # (and of the warm start's energy check) over its own CUDA-event time
@@ -540,7 +549,10 @@ def run_ours(args, envs, desc, batched):
                          "kernel_ms_per_step": kernel_ms / args.steps},
             "e2e": {"value": e2e, "unit": "sim-s/wall-s",
                     "h2d_bytes_per_step": 24 * n_vertices,
-                    "d2h_bytes_per_step": 24 * n_vertices},
+                    "d2h_bytes_per_step": 24 * n_vertices,
+                    "steps": e2e_steps,
+                    "window": "the value's warm-up and timed steps, rerun from the window's "
+                              "first state with host arrays in and out"},
             "gpu_launches": launches}
     if clocks:
         line["clocks"] = clocks
@@ -719,7 +731,8 @@ def main():
     ap.add_argument("--workload", default="batch256")
     ap.add_argument("--mode", default="auto",
                     choices=["auto", "block", "graph", "hostloop", "persist"])
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="timed end-to-end steps (0 = --steps)")
     ap.add_argument("--secondary-steps", type=int, default=30)
     ap.add_argument("--long-steps", type=int, default=1000,
                     help="steps of the whole-trajectory plain / warm-started batch comparison")
