@@ -928,9 +928,10 @@ int upload_plan(vbd_solver* s, const int* iters) {
 // Neighbour lists of the persistent kernel's readiness waits (PersistNbr):
 // for every block b and colour c, the other blocks that own a solved vertex
 // sharing a tet with one of b's colour-c vertices.  The owner of a vertex
-// follows persist_kernel's assignment exactly: colour c's chunk q goes to
-// block ((q - chunk_begin) / warps per block) mod span, span = every block,
-// or the first nsb blocks for a small colour.
+// follows persist_kernel's assignment exactly: a large colour's chunk q goes
+// to block ((q - chunk_begin) / warps per block) mod (every block), a small
+// colour's to block (q - chunk_begin) mod nsb, nsb = the largest small
+// colour's chunk count.
 void build_persist_neighbours(const Layout& L, int tpv, int nwarps, int nb, std::vector<int>& off,
                               std::vector<int>& idx) {
   const EnvInfo& e = L.env[0];
@@ -940,16 +941,18 @@ void build_persist_neighbours(const Layout& L, int tpv, int nwarps, int nb, std:
   for (int c = 0; c < C; ++c) {
     const ColorInfo& ci = L.color[e.cbase + c];
     const int nch = ci.chunk_end - ci.chunk_begin;
-    if (is_small(nch)) nsb = std::max(nsb, (nch + nwarps - 1) / nwarps);
+    if (is_small(nch)) nsb = std::max(nsb, nch);
   }
   nsb = std::min(nsb, nb);
   std::vector<int> owner(e.nsolved, -1);
   auto for_each_vertex = [&](auto&& f) {
     for (int c = 0; c < C; ++c) {
       const ColorInfo& ci = L.color[e.cbase + c];
-      const int span = is_small(ci.chunk_end - ci.chunk_begin) ? nsb : nb;
+      const bool small = is_small(ci.chunk_end - ci.chunk_begin);
       for (int q = ci.chunk_begin; q < ci.chunk_end; ++q) {
-        const int b = ((q - ci.chunk_begin) / nwarps) % span;
+        // a small colour: chunk k on block k mod nsb (its warps split it);
+        // a large one: chunks in groups of nwarps, group g on block g mod nb
+        const int b = small ? (q - ci.chunk_begin) % nsb : ((q - ci.chunk_begin) / nwarps) % nb;
         for (int vi = 0; vi < cpw; ++vi) {
           const int gv = ci.vbegin + (q - ci.chunk_begin) * cpw + vi;
           if (gv < ci.vend) f(c, q, vi, gv - e.vbase, b);

@@ -13,8 +13,9 @@
 //             and update their vertices (process_chunk).  Small colours (at
 //             most kPersistSmallBlocks blocks' worth of chunks, e.g. the
 //             107-vertex colours of a voxel cantilever) are done by the
-//             first S blocks only (S = blocks the largest small colour
-//             needs).  Colours are separated by neighbour-scoped readiness
+//             first S blocks only (S = the largest small colour's chunk
+//             count), one chunk per block, its slot steps split over the
+//             block's warps.  Colours are separated by neighbour-scoped readiness
 //             (PersistNbr, vbd_persist.h): a block waits only for the blocks
 //             that own vertices sharing a tet with its own vertices of the
 //             colour.  Without neighbour lists: a grid barrier between
@@ -190,6 +191,9 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
   __shared__ double s_dsum[16];
   __shared__ double s_total;
   __shared__ int s_ok;
+  // per-part sums of a small colour's chunk (see the sweep loop)
+  constexpr int kPartFloats = SplitBuf<TPV>::per_part;
+  __shared__ Real s_split[Prefetch<TPV>::steps * kPartFloats];
   const StepConst sc = make_const(*pp);
   const double tol = pp->tol;
   const int max_iter = pp->max_iter;
@@ -312,16 +316,21 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
       VBD_GRID_SYNC();
     }
   }
-  // small colours run on the first nsb blocks: as many as the largest of
-  // them needs for one chunk per warp
+  // small colours run on the first nsb blocks, one chunk per block at a time
+  // (as many blocks as the largest of them has chunks): the block's warps
+  // split the chunk's slot steps (process_chunk_part) and warp 0 adds the
+  // parts in part order -- a small colour's time is one chunk's dependent
+  // chain, so a shorter chain is what shortens it
   auto is_small = [&](int nch) { return nb > 1 && nch <= kPersistSmallBlocks * nwarps; };
   const bool scoped = nb > 1 && nbr.off != nullptr;
   int nsb = 1;
   for (int c = 0; c < e.ncolors; ++c) {
     const int nch = m.color[e.cbase + c].chunk_end - m.color[e.cbase + c].chunk_begin;
-    if (is_small(nch)) nsb = max(nsb, (nch + nwarps - 1) / nwarps);
+    if (is_small(nch)) nsb = max(nsb, nch);
   }
   nsb = min(nsb, nb);
+  constexpr int kParts = Prefetch<TPV>::steps;  // parts per chunk at most
+  const int W = min(nwarps, kParts);
   unsigned long long sub_bar = 0ull;  // arrivals that complete the next small-colour barrier
   int it = 0;
   bool conv = false, nan = false;
@@ -339,11 +348,25 @@ __global__ void __launch_bounds__(512) persist_kernel(DevMesh m,
         if (threadIdx.x == 0) atomicOr(m.status, kStatTimeout);
         return;
       }
-      if (blockIdx.x < span)
+      if (small) {
+        if (blockIdx.x < span)
+          for (int q = ci.chunk_begin + blockIdx.x; q < ci.chunk_end; q += span) {
+            if (warp < W)
+              process_chunk_part<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, stat,
+                                                             tab, warp, W,
+                                                             s_split + warp * kPartFloats);
+            __syncthreads();
+            if (warp == 0)
+              finish_split_chunk<Real, SReal, TPV>(m, e.vbase, ci, q, lane, state, sc, cmax,
+                                                   stat, dxrec, s_split, W);
+            __syncthreads();  // s_split is rewritten by the next chunk
+          }
+      } else if (blockIdx.x < span) {
         for (int q = ci.chunk_begin + blockIdx.x * nwarps + warp; q < ci.chunk_end;
              q += span * nwarps)
           process_chunk<Real, SReal, TPV, MAT, FMT>(m, e.vbase, ci, q, lane, state, sc, cmax,
                                                     stat, tab, dxrec);
+      }
       if (c + 1 == e.ncolors) break;
       if (scoped) {
         publish_epoch(nbr, phase + 1);
